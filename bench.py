@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Throughput of the fused near-field SAR backprojection + surface-normal vote.
+
+Workload (one "step"): the 128^3-voxel, 128x128-antenna, 256-frequency scene
+(2 mm voxel and antenna pitch, 77-81 GHz, 20k scatterers on a box U cylinder at
+z = 0.45 m, 15 dB) -- backprojection fused with the normal vote over the whole grid
+(image + vote), then the mask / unit-normal epilogue.  8.8e12 voxel*antenna*frequency
+updates per step.  Inputs are synthetic (seeded); they are resident in HBM before the
+timed region; the 126 MB L2 is flushed (256 MB write) before every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line on rank 0.  ``--impl reference`` times the reference's own CPU
+imager (src/data_processing/cpp/imaging.cpp, built from source into oracle/_ref) on the
+host cores on a bounded voxel sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "G voxel*antenna*frequency updates/s (fused image + normal vote, mixed FP64/FP32)"
+UNIT = "G updates/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU seconds of the bounded reference/CPU sample")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="mmn_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        loaded = sorted(sm)[len(sm) // 4:] if len(sm) >= 4 else sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows
+                                   if r[3].replace(".", "").isdigit()) if rows else None}
+
+
+# --------------------------------------------------------------------- the scene
+def load_scene(device):
+    from mmnorm_b200 import scenes
+    return scenes.config1(sign=-1, device=device)
+
+
+def cpu_sample_axes(sc, n_voxels_target, cores):
+    """A voxel sub-grid of the workload's grid: `cores` x-slices (the reference imager's
+    OpenMP loop runs over x) spread over the grid, one y row, z columns as needed."""
+    nx = max(1, min(len(sc.x_locs), cores))
+    xi = np.linspace(0, len(sc.x_locs) - 1, nx).round().astype(int)
+    nz = max(1, min(len(sc.z_locs), int(math.ceil(n_voxels_target / nx))))
+    zi = np.linspace(0, len(sc.z_locs) - 1, nz).round().astype(int)
+    yi = np.array([len(sc.y_locs) // 2])
+    return sc.x_locs[xi], sc.y_locs[yi], sc.z_locs[zi]
+
+
+def time_reference_imager(sc, steps, warmup, target_seconds):
+    """Reference imager on host cores; returns (updates/s, info dict)."""
+    from oracle import ref_imager
+    cores = os.cpu_count() or 1
+    A, F = sc.meas.shape
+    meas = sc.meas[:, :, None]
+    rxo = np.zeros((1, 3), np.float32)
+    # calibrate: one voxel per x-slice
+    x, y, z = cpu_sample_axes(sc, cores, cores)
+    cal = ref_imager.time_sample(x, y, z, sc.antenna_locs, meas, rxo, sc.slope, sc.f_lo,
+                                 steps=1, warmup=0, threads=cores)
+    per = max(1e-6, cal["step_seconds"][0] - cal["conversion_seconds"])
+    nvox_cal = len(x) * len(y) * len(z)
+    n_target = int(nvox_cal * target_seconds / per)
+    x, y, z = cpu_sample_axes(sc, max(nvox_cal, n_target), cores)
+    res = ref_imager.time_sample(x, y, z, sc.antenna_locs, meas, rxo, sc.slope, sc.f_lo,
+                                 steps=steps, warmup=warmup, threads=cores)
+    nvox = len(x) * len(y) * len(z)
+    upd = nvox * A * F
+    compute = [max(1e-9, t - res["conversion_seconds"]) for t in res["step_seconds"]]
+    rate = upd / statistics.median(compute)
+    info = {"voxels": nvox, "updates_per_step": upd, "step_seconds": res["step_seconds"],
+            "conversion_seconds": res["conversion_seconds"], "threads": res["threads"],
+            "sample": "%d voxels (%d x-slices x %d y x %d z) of the 128^3 grid, all %d antennas "
+                      "x %d freqs; reference imager (imaging.cpp) built from source, "
+                      "OMP_NUM_THREADS=%d; rate excludes the per-call pybind11 input "
+                      "conversion (%.2f s, timed on a 1-voxel call)"
+                      % (nvox, len(x), len(y), len(z), A, F, res["threads"],
+                         res["conversion_seconds"])}
+    return rate, info
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    try:
+        from oracle import ref_imager
+        if not ref_imager.available():
+            from oracle import build as ob
+            ob.build_ref()
+        if not ref_imager.available():
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "reference imager not built (oracle/build.py needs the mmNorm "
+                              "checkout at build time)"}))
+            return 0
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": str(e)[:200]}))
+        return 0
+    sc = load_scene("cuda" if _has_cuda() else None)
+    per_step = max(2.0, args.cpu_seconds / 3.0)
+    rate, info = time_reference_imager(sc, max(1, args.steps), max(0, args.warmup), per_step)
+    value = rate / 1e9
+    ms = 1e3 * statistics.median(info["step_seconds"])
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded point-scatterer scene)",
+        "config": {"workload": sc.name + " (128^3 voxels @2 mm, 128x128 antennas @2 mm, "
+                   "256 freqs 77-81 GHz)", "voxels": sc.num_voxels,
+                   "antennas": int(sc.meas.shape[0]), "freqs": int(sc.meas.shape[1]),
+                   "parallelism": "host OpenMP", "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["threads"],
+                         "kind": "reference", "sample": info["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def _has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+# ------------------------------------------------------------------- our arm
+def ours_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    from mmnorm_b200 import _lib, ops
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=dev)
+    lib = _lib.load()
+    _lib.check(lib.mmn_check_device(local), "mmn_check_device")
+
+    sc = load_scene(dev)
+    A, F = sc.meas.shape
+    V = sc.num_voxels
+    updates = V * A * F
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    xs, ys, zs = t(sc.x_locs), t(sc.y_locs), t(sc.z_locs)
+    ant, rxo = t(sc.antenna_locs), t(np.zeros((1, 3), np.float32))
+    meas = t(sc.meas)
+    prob = ops.make_problem(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope)
+    ws = torch.empty(ops.workspace_bytes(prob, "mixed"), dtype=torch.uint8, device=dev)
+    plan = ops.plan_info(prob, "mixed")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(mode="mixed", ev=None):
+        flush.fill_(1)
+        if ev is not None:
+            ev[0].record(stream)
+        img, vote = ops.backproject(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope,
+                                    mode=mode, workspace=ws)
+        if ev is not None:
+            ev[1].record(stream)
+        normals, mask = ops.surface_normals(img, vote, 0.05)
+        return img, vote, normals, mask
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # FP32 peak probe (the roofline denominator), right before the timed region
+    probe_out = torch.empty(148 * 8 * 256, dtype=torch.float32, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks, iters = sms * 8, 20000
+    for _ in range(2):
+        _lib.check(lib.mmn_fp32_peak_probe(blocks, 200, ops._vp(probe_out), ops._stream(dev)),
+                   "probe")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    probe_rates = []
+    for _ in range(3):
+        e0.record(stream)
+        _lib.check(lib.mmn_fp32_peak_probe(blocks, iters, ops._vp(probe_out), ops._stream(dev)),
+                   "probe")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        probe_rates.append(blocks * 256.0 * iters * 32 / (e0.elapsed_time(e1) * 1e-3))
+    fp32_peak = max(probe_rates)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    clocks = ClockSampler(local)
+    kernel_events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                     for _ in range(args.steps)]
+    barrier()
+    clocks.start()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        step(ev=kernel_events[k])
+    t1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    total_ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = world * updates * args.steps / (total_ms * 1e-3) / 1e9
+    kern_ms = [a.elapsed_time(b) for a, b in kernel_events]
+    kern_avg_s = statistics.mean(kern_ms) * 1e-3
+    launches_per_step = 4 + (1 if plan["splits"] > 1 else 0)
+
+    out = {}
+    if rank == 0 and world == 1 and args.plain_steps > 0:
+        # plain FP32 sincos-per-sample form on the same workload
+        step("plain")
+        pe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.plain_steps)]
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for k in range(args.plain_steps):
+            step("plain", ev=pe[k])
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1) / args.plain_steps
+        pval = updates / (pms * 1e-3) / 1e9
+        out["plain"] = {"value": pval, "unit": UNIT, "ms_per_step": pms,
+                        "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in pe),
+                        "mixed_over_plain": value / pval}
+
+    # end to end through the public API: pinned host inputs -> device -> image + normals
+    # -> pinned host outputs, every step
+    e2e = None
+    if rank == 0:
+        h_meas = torch.empty(meas.shape, dtype=meas.dtype, pin_memory=True)
+        h_meas.copy_(torch.as_tensor(sc.meas))
+        h_ant = torch.as_tensor(sc.antenna_locs).pin_memory()
+        h_axes = [torch.as_tensor(a).pin_memory() for a in (sc.x_locs, sc.y_locs, sc.z_locs)]
+        h_rxo = torch.zeros((1, 3), dtype=torch.float32).pin_memory()
+        h_img = torch.empty(V, dtype=torch.complex64, pin_memory=True)
+        h_nrm = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
+        n_e2e = max(1, min(args.steps, 3))
+
+        def e2e_step():
+            flush.fill_(1)
+            d_meas = h_meas.to(dev, non_blocking=True)
+            d_ant = h_ant.to(dev, non_blocking=True)
+            d_axes = [a.to(dev, non_blocking=True) for a in h_axes]
+            d_rxo = h_rxo.to(dev, non_blocking=True)
+            img, vote = ops.backproject(*d_axes, d_ant, d_rxo, d_meas, sc.wavelength, sc.slope,
+                                        mode="mixed")
+            normals, mask = ops.surface_normals(img, vote, 0.05)
+            h_img.copy_(img.reshape(-1), non_blocking=True)
+            h_nrm.copy_(normals.reshape(-1, 3), non_blocking=True)
+            torch.cuda.synchronize()
+
+        e2e_step()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record(stream)
+        for _ in range(n_e2e):
+            e2e_step()
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ems = s0.elapsed_time(s1) / n_e2e
+        h2d = (h_meas.numel() * 8 + h_ant.numel() * 4 + sum(a.numel() for a in h_axes) * 4
+               + h_rxo.numel() * 4)
+        d2h = h_img.numel() * 8 + h_nrm.numel() * 4
+        e2e = {"value": updates / (ems * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ems,
+               "path": "pinned host -> ops.backproject + ops.surface_normals (C ABI) -> "
+                       "pinned host image + unit normals"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import ref_imager
+            if ref_imager.available():
+                rate, info = time_reference_imager(sc, 1, 0, args.cpu_seconds)
+                cpu = {"value": rate / 1e9, "unit": UNIT, "cores": info["threads"],
+                       "kind": "reference", "sample": info["sample"]}
+        except Exception as e:  # pragma: no cover
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": "failed: %s" % str(e)[:200]}
+
+    if rank == 0:
+        flops = 8.0 * updates          # one complex multiply-add (4 FFMA) per update
+        achieved = flops / kern_avg_s / 1e12
+        peak = fp32_peak / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "precision": "mixed: FP64 range and phase wrap, FP32 Horner rotation recurrence "
+                         "re-anchored every 32 samples, FP32 accumulation",
+            "data": "synthetic (seeded point-scatterer scene, exp(-j4pi f r/c)/r^2, 15 dB)",
+            "config": {"workload": sc.name + " (128^3 voxels @2 mm, 128x128 antennas @2 mm, "
+                       "256 freqs 77-81 GHz; image + vote + unit normals)",
+                       "voxels": V, "antennas": A, "freqs": F,
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "flushed before every step (256 MB write)",
+                       "plan": plan},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": _read_traffic(),
+                         "kernel": "bp_fwd_kernel<4,128,mixed>",
+                         "flops_per_update": 8,
+                         "peak_source": "FP32 FFMA probe (mmn_fp32_peak_probe) timed in this "
+                                        "run; MEASURED_PEAKS.json has no FP32 figure",
+                         "kernel_ms": statistics.mean(kern_ms)},
+            "clocks": clk,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "cpu_baseline": cpu,
+        }
+        line.update(out)
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _read_traffic():
+    """DRAM bytes per launch of the forward kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "bp_fwd_mixed_boxcyl128.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

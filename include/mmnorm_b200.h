@@ -1,0 +1,176 @@
+/*
+ * mmnorm_b200.h -- C ABI of the B200 (sm_100a) near-field SAR backprojection and
+ * mmWave surface-normal vote.
+ *
+ * Every pointer argument is a DEVICE pointer unless the name ends in _host.  Every
+ * entry point is asynchronous on the given stream, allocates nothing unless stated,
+ * and returns MMN_OK or an MMN_ERR_* code; no C++ exception crosses this boundary.
+ * Calls on distinct streams with distinct workspaces are thread-safe.
+ *
+ * Conventions shared with the reference (src/data_processing/cuda/imaging_gpu.cu):
+ *   - voxel (x, y, z) has flat index  x*NY*NZ + y*NZ + z                (:121-122)
+ *   - virtual antenna i has TX position antenna_locs[i] and RX position
+ *     antenna_locs[i] + rx_offsets[i % num_rx]                           (:67-83)
+ *   - round-trip distance d = |v - tx| + |v - rx|, plus 0.15 m if is_ti_radar (:86-88)
+ *   - full matched filter: sum_j m[i,j] exp(-j 2 pi d (1/wavelength + j slope/c)) (:112)
+ *   - interpolated mode: m_fft[i, floor(d/fft_spacing/2)] exp(-j 2 pi d/wavelength),
+ *     skipped when d < 0 or d > fft_spacing * num_bins                   (:90-105)
+ *   - normal vote: sum_i Re(c_i conj(I))/|I| (tx_i + o_i/2 - v)
+ *     (src/data_processing/cuda/surface_normal_est.cu:128-145)
+ * Complex arrays are interleaved (re, im) float32 pairs, i.e. complex64.
+ */
+#ifndef MMNORM_B200_H
+#define MMNORM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MMN_OK 0
+#define MMN_ERR_INVALID_ARGUMENT 1 /* bad size, mode or flag                   */
+#define MMN_ERR_NULL_POINTER 2     /* a required pointer is NULL               */
+#define MMN_ERR_UNSUPPORTED 3      /* device is not sm_100 / feature missing   */
+#define MMN_ERR_WORKSPACE 4        /* workspace NULL, misaligned or too small  */
+#define MMN_ERR_CUDA 5             /* a CUDA runtime call failed               */
+#define MMN_ERR_TIMEOUT 6          /* a bounded in-kernel wait gave up         */
+#define MMN_ERR_TOO_LARGE 7        /* a size exceeds a documented maximum      */
+
+/* forward-projection forms */
+#define MMN_MODE_MIXED 0  /* FP64 range + wrap, FP32 rotation recurrence (default)  */
+#define MMN_MODE_PLAIN 1  /* FP32 range and phase, one sincosf per sample           */
+#define MMN_MODE_INTERP 2 /* reference interpolated mode (range-FFT bin + 1 phasor) */
+
+/* Problem description.  All array pointers are device pointers. */
+typedef struct mmn_problem {
+    int32_t num_x, num_y, num_z;  /* voxel grid                                   */
+    const float *x_locs;          /* [num_x] voxel centres along x                */
+    const float *y_locs;          /* [num_y]                                      */
+    const float *z_locs;          /* [num_z]                                      */
+    int32_t num_antennas;         /* virtual antennas A*R (TX repeated per RX)    */
+    int32_t num_rx;               /* R >= 1                                       */
+    const float *antenna_locs;    /* [num_antennas, 3] TX positions               */
+    const float *rx_offsets;      /* [num_rx, 3]                                  */
+    const float *pos_offsets;     /* [num_antennas, 3] added to TX and RX, or NULL */
+    int32_t num_samples;          /* F samples (full) or range bins (interp)      */
+    const float *meas;            /* complex64 [num_antennas, num_samples]        */
+    double wavelength;            /* c / start frequency                          */
+    double slope;                 /* Hz per sample                                */
+    double fft_spacing;           /* interpolated mode only                       */
+    int32_t is_ti_radar;          /* add 0.15 m to the round-trip distance        */
+    int32_t reserved;
+} mmn_problem;
+
+/* Library identification and device check (0 when device `dev` is an sm_100 part). */
+const char *mmn_version(void);
+int mmn_check_device(int dev);
+
+/* Bytes of device workspace mmn_backproject needs for `p` in `mode` (256-aligned).
+ * Returns 0 for an invalid problem.  Depends on the current device (occupancy). */
+size_t mmn_workspace_bytes(const mmn_problem *p, int32_t mode, int32_t want_vote);
+
+/* Kernel variants of the full-mode forward pass (voxels per thread x threads per CTA)
+ * for the autotuner; no reference counterpart (the reference has one fixed launch,
+ * block=512, py_image_gpu.py:272-273).  mmn_set_variant selects the process-wide
+ * variant mmn_backproject uses for MMN_MODE_MIXED / MMN_MODE_PLAIN. */
+int mmn_num_variants(int32_t mode);
+int mmn_variant_info(int32_t mode, int32_t idx, int32_t *voxels_per_thread, int32_t *threads);
+int mmn_set_variant(int32_t mode, int32_t idx);
+
+/* The decomposition mmn_backproject will use for `p`: voxel tiles, antenna splits,
+ * antennas per shared-memory stage, threads per CTA, voxels per thread. */
+int mmn_plan_info(const mmn_problem *p, int32_t mode, int32_t *tiles, int32_t *splits,
+                  int32_t *ant_per_stage, int32_t *threads, int32_t *voxels_per_thread);
+
+/*
+ * Fused backprojection + vote.  image: complex64 [V] raw sum over all virtual
+ * antennas and samples (not normalised).  vote (may be NULL): complex64 [3, V], the
+ * plane k holding W_k(v) = sum_i c_i(v) * (tx_i + o_i/2 - v)_k, from which the
+ * reference's normal is Re(conj(I) W)/|I|.  Replaces the cuda_image launch in
+ * src/data_processing/cuda/py_image_gpu.py:189-199 and, for the vote, the
+ * cuda_sn_est launch in src/data_processing/cuda/py_sn_est_gpu.py:229-246.
+ */
+int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vote,
+                    void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/*
+ * Unit surface normals from (image, vote): mask |I| > filter_percent * max|I|
+ * (src/data_processing/cuda/py_sn_est_gpu.py:326), raw normal Re(conj(I) W)/|I|
+ * (surface_normal_est.cu:138-144), unit normalisation (image_processor.py:396).
+ * normals: float32 [V, 3], NaN outside the mask.  mask (may be NULL): uint8 [V].
+ * raw (may be NULL): float32 [V, 3] un-normalised normal, NaN outside the mask.
+ * Needs mmn_normals_workspace_bytes() of workspace.
+ */
+size_t mmn_normals_workspace_bytes(int64_t num_voxels);
+int mmn_normals(int64_t num_voxels, const float *image, const float *vote,
+                float filter_percent, float *normals, uint8_t *mask, float *raw,
+                void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/*
+ * Drop-in for the reference kernel launch `cuda_image`
+ * (src/data_processing/cuda/imaging_gpu.cu:12-21, launched at py_image_gpu.py:189-199):
+ * same arguments in the same order and meaning (SoA measurements, float scalars,
+ * start_ind), plus the launch extent voxel_count (the reference's grid_dim *
+ * threads_per_block, py_image_gpu.py:273,187; -1 = to the end of the grid), a
+ * workspace and a stream.  Writes p_xyz_r/p_xyz_i for voxels [start_ind,
+ * start_ind + voxel_count).  use_interpolated_processing == 0 runs the mixed-precision
+ * matched filter; != 0 runs the interpolated mode with the reference's arithmetic.
+ */
+size_t mmn_cuda_image_workspace_bytes(int num_antennas, int samples_per_meas,
+                                      int use_interpolated_processing);
+/* Exact workspace for one mmn_cuda_image call (includes the antenna-split partial sums,
+ * which depend on the launch extent and the current device). */
+size_t mmn_cuda_image_workspace_bytes_for(int num_x, int num_y, int num_z, int num_antennas,
+                                          int samples_per_meas, int start_ind, int voxel_count,
+                                          int use_interpolated_processing);
+int mmn_cuda_image(float *p_xyz_r, float *p_xyz_i, const float *x_locs,
+                   const float *y_locs, const float *z_locs, const float *antenna_locs,
+                   const float *meas_r, const float *meas_i, const float *rx_offsets,
+                   float slope, float wavelength, float fft_spacing, int num_x,
+                   int num_y, int num_z, int num_antennas, int num_rx_antennas,
+                   int samples_per_meas, int start_ind, int is_ti_radar,
+                   int use_interpolated_processing, int voxel_count, void *workspace,
+                   size_t workspace_bytes, cudaStream_t stream);
+
+/*
+ * Drop-in for the reference kernel launch `cuda_sn_est`
+ * (src/data_processing/cuda/surface_normal_est.cu:14-25, launched at
+ * py_sn_est_gpu.py:229-246): interpolated-mode normal vote for the listed valid
+ * voxels with the reference's arithmetic; writes normals_x/y/z[ind] for
+ * ind in [start_ind, min(num_valid_idx, start_ind + count)) (count = -1: all).
+ */
+size_t mmn_cuda_sn_est_workspace_bytes(int num_antennas, int samples_per_meas);
+int mmn_cuda_sn_est(float *normals_x, float *normals_y, float *normals_z,
+                    const int *valid_idx_x, const int *valid_idx_y,
+                    const int *valid_idx_z, const float *p_xyz_r, const float *p_xyz_i,
+                    const float *x_locs, const float *y_locs, const float *z_locs,
+                    const float *antenna_locs, const float *meas_r, const float *meas_i,
+                    const float *rx_offsets, float slope, float wavelength,
+                    float fft_spacing, int num_x, int num_y, int num_z,
+                    int num_antennas, int num_rx_antennas, int num_valid_idx,
+                    int samples_per_meas, int start_ind, int is_ti_radar, int count,
+                    void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/*
+ * FP32 FMA throughput probe (no counterpart in the reference): `blocks` CTAs of 256
+ * threads each run 16 independent FFMA chains for `iters` iterations, i.e.
+ * blocks*256*iters*32 FLOPs; out: float [blocks*256] sink.  Timed by the caller, it gives
+ * the measured FP32 peak that bounds the forward kernels.
+ */
+int mmn_fp32_peak_probe(int blocks, int iters, float *out, cudaStream_t stream);
+
+/*
+ * Status word that kernels set when a bounded wait gives up (MMN_ERR_TIMEOUT) -- kept in
+ * the first bytes of every workspace.  Synchronises `stream`, copies the word to the
+ * host, and clears it.  Returns MMN_OK or the CUDA error; *status receives the word.
+ */
+int mmn_read_status(void *workspace, int32_t *status, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MMNORM_B200_H */

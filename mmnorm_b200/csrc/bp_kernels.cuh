@@ -1,0 +1,88 @@
+// bp_kernels.cuh -- kernel parameter blocks and launch helpers shared by the
+// kernel files and the C ABI (capi.cu).
+#pragma once
+#include "mmn_internal.cuh"
+
+namespace mmn {
+
+// ------------------------------------------------------------- full-mode forward
+struct FwdParams {
+    const float *x_locs, *y_locs, *z_locs;
+    int32_t nx, ny, nz;
+    int64_t nvox;          // voxels in the whole grid
+    int64_t vox_start;     // first voxel of this launch
+    int64_t vox_count;     // voxels in this launch (tiles cover [vox_start, +vox_count))
+    const AntRec *ant;     // [num_ant]
+    const float2 *meas;    // [num_ant, fp] complex64, fp % 32 == 0, 16-byte aligned
+    int32_t num_ant;
+    int32_t fp;
+    int32_t ant_per_stage; // antennas per shared-memory stage
+    int32_t pad1;
+    const int32_t *mono_flag; // device word: 1 when all RX offsets are zero
+    double k0, kd;         // 2*pi/lambda, 2*pi*slope/c
+    double ti;             // 0.15 or 0
+    int32_t num_tiles;
+    int32_t num_splits;
+    int32_t ant_per_split;
+    int32_t pad0;
+    float2 *image;         // [nvox] complex64 or null
+    float2 *vote;          // [3, nvox] or null
+    float *out_r, *out_i;  // [nvox] SoA image (reference layout) or null
+    float4 *partial;       // [num_splits, vox_count, 2] (num_splits > 1)
+    int32_t *status;
+};
+
+struct FwdVariant {
+    int t;      // voxels per thread
+    int nt;     // threads per CTA
+    bool plain; // PLAIN form
+    const void *fn;
+};
+
+const FwdVariant *fwd_variants(int *count);
+cudaError_t launch_fwd(const FwdVariant &var, const FwdParams &p, size_t smem,
+                       cudaStream_t stream);
+cudaError_t launch_reduce(const FwdParams &p, cudaStream_t stream);
+cudaError_t launch_prep_antennas(const float *ant, const float *rxo, int R, const float *pos_off,
+                                 int A, AntRec *out, int32_t *mono_flag, cudaStream_t stream);
+cudaError_t launch_pad_meas(const float2 *src, int A, int F, float2 *dst, int Fp,
+                            cudaStream_t stream);
+cudaError_t launch_interleave_pad(const float *re, const float *im, int A, int F, float2 *dst,
+                                  int Fp, cudaStream_t stream);
+
+// ---------------------------------------------------------- interpolated mode
+struct InterpParams {
+    const float *x_locs, *y_locs, *z_locs;
+    int32_t nx, ny, nz;
+    int32_t num_ant, num_rx, nbins;
+    const float *ant;        // [num_ant, 3]
+    const float *rxo;        // [num_rx, 3]
+    const float2 *meas;      // complex64 [num_ant, nbins] (or null when SoA is used)
+    const float *meas_r;     // SoA planes (reference layout) or null
+    const float *meas_i;
+    float fft_spacing, wavelength;
+    int32_t is_ti;
+    int32_t pad0;
+    // image pass: voxels [start, start + count)
+    int64_t start, count;
+    float *out_r, *out_i;    // SoA outputs (reference layout) or null
+    float2 *image;           // complex64 output or null
+    float2 *vote;            // fused vote [3, V] (image pass) or null
+    int64_t nvox;
+    // normal pass (cuda_sn_est): valid voxel lists
+    const int *vidx_x, *vidx_y, *vidx_z;
+    const float *img_r, *img_i;
+    float *n_x, *n_y, *n_z;
+    int32_t num_valid;
+    int32_t pad1;
+};
+
+cudaError_t launch_interp_image(const InterpParams &p, cudaStream_t stream);
+cudaError_t launch_interp_normals(const InterpParams &p, cudaStream_t stream);
+
+// --------------------------------------------------------------------- epilogue
+cudaError_t launch_normals(int64_t nvox, const float2 *image, const float2 *vote,
+                           float filter_percent, float *normals, uint8_t *mask, float *raw,
+                           unsigned int *max_bits, cudaStream_t stream);
+
+}  // namespace mmn

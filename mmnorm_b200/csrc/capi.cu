@@ -1,0 +1,531 @@
+// capi.cu -- extern "C" entry points declared in include/mmnorm_b200.h.
+//
+// Host-side planning for the fused forward pass:
+//   * measurement rows are padded to Fp = roundup(F, 32) samples (zero samples add
+//     nothing) and must sit 16-byte aligned for the bulk copies, else they are copied
+//     into the workspace;
+//   * antennas per shared-memory stage = 48 KB / (64 + 8*Fp), at most 16;
+//   * voxel tiles of NT*T voxels; when there are too few tiles to fill the GPU, the
+//     antenna range is split S ways (S chosen by a wave-quantisation cost model over
+//     the occupancy-derived CTA slots) and the S partial sums are reduced in split order.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+
+#include "bp_kernels.cuh"
+
+using namespace mmn;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+constexpr int kMaxStageBytes = 48 * 1024;
+constexpr int kMaxFp = 24576;  // one antenna row per stage still fits in shared memory
+
+inline size_t align_up(size_t x, size_t a = kAlign) { return (x + a - 1) / a * a; }
+
+std::atomic<int> g_variant[2] = {{0}, {4}};  // default variant per MIXED / PLAIN
+
+struct FwdPlan {
+    const FwdVariant *var;
+    int fp, ant_per_stage, tiles, splits, ant_per_split;
+    size_t smem;
+    int64_t vox_start, vox_count;
+    bool copy_meas;
+    size_t off_ant, off_meas, off_partial, total;
+};
+
+int variant_index_for(int mode) { return g_variant[mode == MMN_MODE_PLAIN ? 1 : 0].load(); }
+
+int check_problem(const mmn_problem *p, int mode) {
+    if (!p) return MMN_ERR_NULL_POINTER;
+    if (mode != MMN_MODE_MIXED && mode != MMN_MODE_PLAIN && mode != MMN_MODE_INTERP)
+        return MMN_ERR_INVALID_ARGUMENT;
+    if (p->num_x < 1 || p->num_y < 1 || p->num_z < 1) return MMN_ERR_INVALID_ARGUMENT;
+    if (p->num_antennas < 0 || p->num_rx < 1 || p->num_samples < 1)
+        return MMN_ERR_INVALID_ARGUMENT;
+    if (!(p->wavelength > 0.0) || !std::isfinite(p->wavelength) || !std::isfinite(p->slope))
+        return MMN_ERR_INVALID_ARGUMENT;
+    if (mode == MMN_MODE_INTERP && !(p->fft_spacing > 0.0)) return MMN_ERR_INVALID_ARGUMENT;
+    if (!p->x_locs || !p->y_locs || !p->z_locs) return MMN_ERR_NULL_POINTER;
+    if (p->num_antennas > 0 && (!p->antenna_locs || !p->rx_offsets || !p->meas))
+        return MMN_ERR_NULL_POINTER;
+    return MMN_OK;
+}
+
+int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int F, int mode,
+                 bool meas_aligned, bool want_partial_space, FwdPlan *pl) {
+    int nvar = 0;
+    const FwdVariant *vars = fwd_variants(&nvar);
+    int vi = variant_index_for(mode);
+    if (vi < 0 || vi >= nvar || vars[vi].plain != (mode == MMN_MODE_PLAIN))
+        vi = (mode == MMN_MODE_PLAIN) ? 4 : 0;
+    pl->var = &vars[vi];
+    pl->fp = (F + kBlockF - 1) / kBlockF * kBlockF;
+    if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
+    const int rec = (int)sizeof(AntRec) + pl->fp * (int)sizeof(float2);
+    pl->ant_per_stage = std::max(1, std::min(16, kMaxStageBytes / rec));
+    pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec + (pl->var->plain ? pl->fp * 4 : 0);
+    pl->vox_start = vox_start;
+    pl->vox_count = vox_count;
+    const int64_t per_tile = (int64_t)pl->var->nt * pl->var->t;
+    const int64_t tiles = (vox_count + per_tile - 1) / per_tile;
+    if (tiles > (int64_t)1 << 30) return MMN_ERR_TOO_LARGE;
+    pl->tiles = (int)std::max<int64_t>(1, tiles);
+
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (pl->smem > 48 * 1024)
+        cudaFuncSetAttribute(pl->var->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)pl->smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->var->fn, pl->var->nt,
+                                                      pl->smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int64_t slots = (int64_t)sms * per_sm;
+    // split count: minimise waves * antennas-per-CTA, with a 2 % charge per extra split
+    int best_s = 1;
+    double best_cost = 1e300;
+    const int max_s = std::max(1, std::min(64, (A + pl->ant_per_stage - 1) / pl->ant_per_stage));
+    for (int s = 1; s <= max_s; ++s) {
+        const int64_t ctas = (int64_t)pl->tiles * s;
+        const double waves = (double)((ctas + slots - 1) / slots);
+        const double cost = waves * std::ceil((double)A / s) * (1.0 + 0.02 * (s - 1));
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best_s = s;
+        }
+        if (ctas >= 8 * slots) break;
+    }
+    pl->splits = best_s;
+    pl->ant_per_split = A > 0 ? (A + best_s - 1) / best_s : 0;
+    // keep whole stages per split when possible (fewer partial stages)
+    if (best_s > 1) {
+        int aps = (pl->ant_per_split + pl->ant_per_stage - 1) / pl->ant_per_stage * pl->ant_per_stage;
+        pl->ant_per_split = aps;
+        pl->splits = (A + aps - 1) / aps;
+    }
+    pl->copy_meas = !meas_aligned || pl->fp != F;
+    size_t off = kStatusBytes;
+    pl->off_ant = off;
+    off = align_up(off + (size_t)A * sizeof(AntRec));
+    pl->off_meas = off;
+    if (pl->copy_meas) off = align_up(off + (size_t)A * pl->fp * sizeof(float2));
+    pl->off_partial = off;
+    if (pl->splits > 1 || want_partial_space)
+        off = align_up(off + (size_t)pl->splits * (size_t)vox_count * 8 * sizeof(float));
+    pl->total = off;
+    return MMN_OK;
+}
+
+int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
+                const float *meas_i, float2 *image, float2 *vote, float *out_r, float *out_i,
+                unsigned char *ws, cudaStream_t stream) {
+    const int A = p->num_antennas;
+    const int F = p->num_samples;
+    cudaError_t e = cudaMemsetAsync(ws, 0, 16, stream);
+    if (e != cudaSuccess) return MMN_ERR_CUDA;
+    AntRec *ant = reinterpret_cast<AntRec *>(ws + pl.off_ant);
+    int32_t *hdr = reinterpret_cast<int32_t *>(ws);
+    e = launch_prep_antennas(p->antenna_locs, p->rx_offsets, p->num_rx, p->pos_offsets, A, ant,
+                             hdr + 1, stream);
+    if (e != cudaSuccess) return MMN_ERR_CUDA;
+    const float2 *meas = reinterpret_cast<const float2 *>(p->meas);
+    if (meas_r) {
+        float2 *dst = reinterpret_cast<float2 *>(ws + pl.off_meas);
+        e = launch_interleave_pad(meas_r, meas_i, A, F, dst, pl.fp, stream);
+        meas = dst;
+    } else if (pl.copy_meas) {
+        float2 *dst = reinterpret_cast<float2 *>(ws + pl.off_meas);
+        e = launch_pad_meas(meas, A, F, dst, pl.fp, stream);
+        meas = dst;
+    }
+    if (e != cudaSuccess) return MMN_ERR_CUDA;
+
+    FwdParams fp;
+    std::memset(&fp, 0, sizeof(fp));
+    fp.x_locs = p->x_locs;
+    fp.y_locs = p->y_locs;
+    fp.z_locs = p->z_locs;
+    fp.nx = p->num_x;
+    fp.ny = p->num_y;
+    fp.nz = p->num_z;
+    fp.nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    fp.vox_start = pl.vox_start;
+    fp.vox_count = pl.vox_count;
+    fp.ant = ant;
+    fp.meas = meas;
+    fp.num_ant = A;
+    fp.fp = pl.fp;
+    fp.ant_per_stage = pl.ant_per_stage;
+    fp.mono_flag = hdr + 1;
+    fp.k0 = 2.0 * kPi / p->wavelength;
+    fp.kd = 2.0 * kPi * p->slope / kC;
+    fp.ti = p->is_ti_radar ? 0.15 : 0.0;
+    fp.num_tiles = pl.tiles;
+    fp.num_splits = pl.splits;
+    fp.ant_per_split = pl.ant_per_split;
+    fp.image = image;
+    fp.vote = vote;
+    fp.out_r = out_r;
+    fp.out_i = out_i;
+    fp.partial = reinterpret_cast<float4 *>(ws + pl.off_partial);
+    fp.status = hdr;
+    if (pl.smem > 48 * 1024)
+        cudaFuncSetAttribute(pl.var->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)pl.smem);
+    e = launch_fwd(*pl.var, fp, pl.smem, stream);
+    if (e != cudaSuccess) return MMN_ERR_CUDA;
+    if (pl.splits > 1) {
+        e = launch_reduce(fp, stream);
+        if (e != cudaSuccess) return MMN_ERR_CUDA;
+    }
+    return MMN_OK;
+}
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+const char *mmn_version(void) { return "mmnorm_b200 0.1.0 (sm_100a)"; }
+
+int mmn_check_device(int dev) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return MMN_ERR_CUDA;
+    return (prop.major == 10 && prop.minor == 0) ? MMN_OK : MMN_ERR_UNSUPPORTED;
+}
+
+int mmn_num_variants(int32_t mode) {
+    int n = 0;
+    const FwdVariant *v = fwd_variants(&n);
+    int c = 0;
+    for (int i = 0; i < n; ++i) c += (v[i].plain == (mode == MMN_MODE_PLAIN));
+    return c;
+}
+
+int mmn_variant_info(int32_t mode, int32_t idx, int32_t *voxels_per_thread, int32_t *threads) {
+    int n = 0;
+    const FwdVariant *v = fwd_variants(&n);
+    int c = 0;
+    for (int i = 0; i < n; ++i) {
+        if (v[i].plain != (mode == MMN_MODE_PLAIN)) continue;
+        if (c == idx) {
+            if (voxels_per_thread) *voxels_per_thread = v[i].t;
+            if (threads) *threads = v[i].nt;
+            return MMN_OK;
+        }
+        ++c;
+    }
+    return MMN_ERR_INVALID_ARGUMENT;
+}
+
+int mmn_set_variant(int32_t mode, int32_t idx) {
+    if (mode != MMN_MODE_MIXED && mode != MMN_MODE_PLAIN) return MMN_ERR_INVALID_ARGUMENT;
+    int n = 0;
+    const FwdVariant *v = fwd_variants(&n);
+    int c = 0;
+    for (int i = 0; i < n; ++i) {
+        if (v[i].plain != (mode == MMN_MODE_PLAIN)) continue;
+        if (c == idx) {
+            g_variant[mode == MMN_MODE_PLAIN ? 1 : 0].store(i);
+            return MMN_OK;
+        }
+        ++c;
+    }
+    return MMN_ERR_INVALID_ARGUMENT;
+}
+
+size_t mmn_workspace_bytes(const mmn_problem *p, int32_t mode, int32_t want_vote) {
+    (void)want_vote;
+    if (check_problem(p, mode) != MMN_OK) return 0;
+    if (mode == MMN_MODE_INTERP) return kStatusBytes;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    FwdPlan pl;
+    if (plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode, aligned16(p->meas),
+                     false, &pl) != MMN_OK)
+        return 0;
+    return pl.total;
+}
+
+int mmn_plan_info(const mmn_problem *p, int32_t mode, int32_t *tiles, int32_t *splits,
+                  int32_t *ant_per_stage, int32_t *threads, int32_t *voxels_per_thread) {
+    int rc = check_problem(p, mode);
+    if (rc != MMN_OK) return rc;
+    if (mode == MMN_MODE_INTERP) return MMN_ERR_INVALID_ARGUMENT;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    FwdPlan pl;
+    rc = plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode, aligned16(p->meas),
+                      false, &pl);
+    if (rc != MMN_OK) return rc;
+    if (tiles) *tiles = pl.tiles;
+    if (splits) *splits = pl.splits;
+    if (ant_per_stage) *ant_per_stage = pl.ant_per_stage;
+    if (threads) *threads = pl.var->nt;
+    if (voxels_per_thread) *voxels_per_thread = pl.var->t;
+    return MMN_OK;
+}
+
+int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vote,
+                    void *workspace, size_t workspace_bytes, cudaStream_t stream) {
+    int rc = check_problem(p, mode);
+    if (rc != MMN_OK) return rc;
+    if (!image) return MMN_ERR_NULL_POINTER;
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
+        return MMN_ERR_WORKSPACE;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    if (p->num_antennas == 0) {
+        if (cudaMemsetAsync(image, 0, nvox * 8, stream) != cudaSuccess) return MMN_ERR_CUDA;
+        if (vote && cudaMemsetAsync(vote, 0, 3 * nvox * 8, stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+        return MMN_OK;
+    }
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (mode == MMN_MODE_INTERP) {
+        if (workspace_bytes < kStatusBytes) return MMN_ERR_WORKSPACE;
+        if (reinterpret_cast<uintptr_t>(p->meas) & 7u) return MMN_ERR_INVALID_ARGUMENT;
+        if (cudaMemsetAsync(ws, 0, 16, stream) != cudaSuccess) return MMN_ERR_CUDA;
+        InterpParams ip;
+        std::memset(&ip, 0, sizeof(ip));
+        ip.x_locs = p->x_locs;
+        ip.y_locs = p->y_locs;
+        ip.z_locs = p->z_locs;
+        ip.nx = p->num_x;
+        ip.ny = p->num_y;
+        ip.nz = p->num_z;
+        ip.num_ant = p->num_antennas;
+        ip.num_rx = p->num_rx;
+        ip.nbins = p->num_samples;
+        ip.ant = p->antenna_locs;
+        ip.rxo = p->rx_offsets;
+        ip.meas = reinterpret_cast<const float2 *>(p->meas);
+        ip.fft_spacing = (float)p->fft_spacing;
+        ip.wavelength = (float)p->wavelength;
+        ip.is_ti = p->is_ti_radar;
+        ip.start = 0;
+        ip.count = nvox;
+        ip.nvox = nvox;
+        ip.image = reinterpret_cast<float2 *>(image);
+        ip.vote = reinterpret_cast<float2 *>(vote);
+        if (p->pos_offsets) return MMN_ERR_UNSUPPORTED;
+        return launch_interp_image(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+    }
+    FwdPlan pl;
+    rc = plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode, aligned16(p->meas),
+                      false, &pl);
+    if (rc != MMN_OK) return rc;
+    if (workspace_bytes < pl.total) return MMN_ERR_WORKSPACE;
+    return run_forward(pl, p, nullptr, nullptr, reinterpret_cast<float2 *>(image),
+                       reinterpret_cast<float2 *>(vote), nullptr, nullptr, ws, stream);
+}
+
+size_t mmn_normals_workspace_bytes(int64_t num_voxels) {
+    (void)num_voxels;
+    return kStatusBytes;
+}
+
+int mmn_normals(int64_t num_voxels, const float *image, const float *vote, float filter_percent,
+                float *normals, uint8_t *mask, float *raw, void *workspace,
+                size_t workspace_bytes, cudaStream_t stream) {
+    if (num_voxels < 1) return MMN_ERR_INVALID_ARGUMENT;
+    if (!image || !vote) return MMN_ERR_NULL_POINTER;
+    if (!normals && !mask && !raw) return MMN_ERR_NULL_POINTER;
+    if (!workspace || workspace_bytes < kStatusBytes ||
+        (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
+        return MMN_ERR_WORKSPACE;
+    if (!(filter_percent >= 0.f) || !std::isfinite(filter_percent))
+        return MMN_ERR_INVALID_ARGUMENT;
+    unsigned int *max_bits = reinterpret_cast<unsigned int *>(
+        static_cast<unsigned char *>(workspace) + 8);
+    cudaError_t e = launch_normals(num_voxels, reinterpret_cast<const float2 *>(image),
+                                   reinterpret_cast<const float2 *>(vote), filter_percent,
+                                   normals, mask, raw, max_bits, stream);
+    return e == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+}
+
+size_t mmn_cuda_image_workspace_bytes(int num_antennas, int samples_per_meas,
+                                      int use_interpolated_processing) {
+    if (use_interpolated_processing) return kStatusBytes;
+    if (num_antennas < 0 || samples_per_meas < 1) return 0;
+    const int fp = (samples_per_meas + kBlockF - 1) / kBlockF * kBlockF;
+    // header + antenna records + interleaved rows; the partial sums are sized per call
+    // by the launch extent, so report the bound for the largest split count (64) of a
+    // 2^17-voxel launch plus the grid-independent part.  Callers that launch more
+    // voxels should query with mmn_cuda_image_workspace_bytes_for.
+    return align_up(kStatusBytes) + align_up((size_t)num_antennas * sizeof(AntRec)) +
+           align_up((size_t)num_antennas * fp * sizeof(float2));
+}
+
+size_t mmn_cuda_image_workspace_bytes_for(int num_x, int num_y, int num_z, int num_antennas,
+                                          int samples_per_meas, int start_ind, int voxel_count,
+                                          int use_interpolated_processing) {
+    if (use_interpolated_processing) return kStatusBytes;
+    const int64_t nvox = (int64_t)num_x * num_y * num_z;
+    if (nvox < 1 || num_antennas < 0 || samples_per_meas < 1 || start_ind < 0) return 0;
+    int64_t count = voxel_count < 0 ? nvox - start_ind : voxel_count;
+    count = std::min<int64_t>(count, nvox - start_ind);
+    if (count < 1) return kStatusBytes;
+    FwdPlan pl;
+    if (plan_forward(nvox, start_ind, count, num_antennas, samples_per_meas, MMN_MODE_MIXED,
+                     false, false, &pl) != MMN_OK)
+        return 0;
+    return pl.total;
+}
+
+int mmn_cuda_image(float *p_xyz_r, float *p_xyz_i, const float *x_locs, const float *y_locs,
+                   const float *z_locs, const float *antenna_locs, const float *meas_r,
+                   const float *meas_i, const float *rx_offsets, float slope, float wavelength,
+                   float fft_spacing, int num_x, int num_y, int num_z, int num_antennas,
+                   int num_rx_antennas, int samples_per_meas, int start_ind, int is_ti_radar,
+                   int use_interpolated_processing, int voxel_count, void *workspace,
+                   size_t workspace_bytes, cudaStream_t stream) {
+    if (!p_xyz_r || !p_xyz_i || !x_locs || !y_locs || !z_locs) return MMN_ERR_NULL_POINTER;
+    if (num_x < 1 || num_y < 1 || num_z < 1 || num_antennas < 0 || num_rx_antennas < 1 ||
+        samples_per_meas < 1 || start_ind < 0)
+        return MMN_ERR_INVALID_ARGUMENT;
+    if (num_antennas > 0 && (!antenna_locs || !meas_r || !meas_i || !rx_offsets))
+        return MMN_ERR_NULL_POINTER;
+    if (!(wavelength > 0.f)) return MMN_ERR_INVALID_ARGUMENT;
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
+        return MMN_ERR_WORKSPACE;
+    const int64_t nvox = (int64_t)num_x * num_y * num_z;
+    if (start_ind >= nvox) return MMN_OK;
+    int64_t count = voxel_count < 0 ? nvox - start_ind : voxel_count;
+    count = std::min<int64_t>(count, nvox - start_ind);
+    if (count < 1) return MMN_OK;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (num_antennas == 0) {
+        if (cudaMemsetAsync(p_xyz_r + start_ind, 0, count * 4, stream) != cudaSuccess ||
+            cudaMemsetAsync(p_xyz_i + start_ind, 0, count * 4, stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+        return MMN_OK;
+    }
+    if (use_interpolated_processing) {
+        if (workspace_bytes < kStatusBytes) return MMN_ERR_WORKSPACE;
+        if (!(fft_spacing > 0.f)) return MMN_ERR_INVALID_ARGUMENT;
+        InterpParams ip;
+        std::memset(&ip, 0, sizeof(ip));
+        ip.x_locs = x_locs;
+        ip.y_locs = y_locs;
+        ip.z_locs = z_locs;
+        ip.nx = num_x;
+        ip.ny = num_y;
+        ip.nz = num_z;
+        ip.num_ant = num_antennas;
+        ip.num_rx = num_rx_antennas;
+        ip.nbins = samples_per_meas;
+        ip.ant = antenna_locs;
+        ip.rxo = rx_offsets;
+        ip.meas_r = meas_r;
+        ip.meas_i = meas_i;
+        ip.fft_spacing = fft_spacing;
+        ip.wavelength = wavelength;
+        ip.is_ti = is_ti_radar;
+        ip.start = start_ind;
+        ip.count = count;
+        ip.nvox = nvox;
+        ip.out_r = p_xyz_r;
+        ip.out_i = p_xyz_i;
+        return launch_interp_image(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+    }
+    mmn_problem p;
+    std::memset(&p, 0, sizeof(p));
+    p.num_x = num_x;
+    p.num_y = num_y;
+    p.num_z = num_z;
+    p.x_locs = x_locs;
+    p.y_locs = y_locs;
+    p.z_locs = z_locs;
+    p.num_antennas = num_antennas;
+    p.num_rx = num_rx_antennas;
+    p.antenna_locs = antenna_locs;
+    p.rx_offsets = rx_offsets;
+    p.num_samples = samples_per_meas;
+    p.wavelength = (double)wavelength;
+    p.slope = (double)slope;
+    p.is_ti_radar = is_ti_radar;
+    FwdPlan pl;
+    int rc = plan_forward(nvox, start_ind, count, num_antennas, samples_per_meas, MMN_MODE_MIXED,
+                          false, false, &pl);
+    if (rc != MMN_OK) return rc;
+    if (workspace_bytes < pl.total) return MMN_ERR_WORKSPACE;
+    return run_forward(pl, &p, meas_r, meas_i, nullptr, nullptr, p_xyz_r, p_xyz_i, ws, stream);
+}
+
+size_t mmn_cuda_sn_est_workspace_bytes(int num_antennas, int samples_per_meas) {
+    (void)num_antennas;
+    (void)samples_per_meas;
+    return kStatusBytes;
+}
+
+int mmn_cuda_sn_est(float *normals_x, float *normals_y, float *normals_z, const int *valid_idx_x,
+                    const int *valid_idx_y, const int *valid_idx_z, const float *p_xyz_r,
+                    const float *p_xyz_i, const float *x_locs, const float *y_locs,
+                    const float *z_locs, const float *antenna_locs, const float *meas_r,
+                    const float *meas_i, const float *rx_offsets, float slope, float wavelength,
+                    float fft_spacing, int num_x, int num_y, int num_z, int num_antennas,
+                    int num_rx_antennas, int num_valid_idx, int samples_per_meas, int start_ind,
+                    int is_ti_radar, int count, void *workspace, size_t workspace_bytes,
+                    cudaStream_t stream) {
+    (void)slope;
+    (void)workspace;
+    (void)workspace_bytes;
+    if (num_valid_idx < 0 || num_x < 1 || num_y < 1 || num_z < 1 || num_antennas < 0 ||
+        num_rx_antennas < 1 || samples_per_meas < 1 || start_ind < 0)
+        return MMN_ERR_INVALID_ARGUMENT;
+    if (num_valid_idx == 0 || start_ind >= num_valid_idx) return MMN_OK;
+    if (!normals_x || !normals_y || !normals_z || !valid_idx_x || !valid_idx_y ||
+        !valid_idx_z || !p_xyz_r || !p_xyz_i || !x_locs || !y_locs || !z_locs)
+        return MMN_ERR_NULL_POINTER;
+    if (num_antennas > 0 && (!antenna_locs || !meas_r || !meas_i || !rx_offsets))
+        return MMN_ERR_NULL_POINTER;
+    if (!(wavelength > 0.f) || !(fft_spacing > 0.f)) return MMN_ERR_INVALID_ARGUMENT;
+    int64_t n = count < 0 ? (int64_t)num_valid_idx - start_ind : count;
+    n = std::min<int64_t>(n, (int64_t)num_valid_idx - start_ind);
+    InterpParams ip;
+    std::memset(&ip, 0, sizeof(ip));
+    ip.x_locs = x_locs;
+    ip.y_locs = y_locs;
+    ip.z_locs = z_locs;
+    ip.nx = num_x;
+    ip.ny = num_y;
+    ip.nz = num_z;
+    ip.num_ant = num_antennas;
+    ip.num_rx = num_rx_antennas;
+    ip.nbins = samples_per_meas;
+    ip.ant = antenna_locs;
+    ip.rxo = rx_offsets;
+    ip.meas_r = meas_r;
+    ip.meas_i = meas_i;
+    ip.fft_spacing = fft_spacing;
+    ip.wavelength = wavelength;
+    ip.is_ti = is_ti_radar;
+    ip.start = start_ind;
+    ip.count = n;
+    ip.vidx_x = valid_idx_x;
+    ip.vidx_y = valid_idx_y;
+    ip.vidx_z = valid_idx_z;
+    ip.img_r = p_xyz_r;
+    ip.img_i = p_xyz_i;
+    ip.n_x = normals_x;
+    ip.n_y = normals_y;
+    ip.n_z = normals_z;
+    ip.num_valid = num_valid_idx;
+    return launch_interp_normals(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+}
+
+int mmn_read_status(void *workspace, int32_t *status, cudaStream_t stream) {
+    if (!workspace || !status) return MMN_ERR_NULL_POINTER;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return MMN_ERR_CUDA;
+    int32_t s = 0;
+    if (cudaMemcpy(&s, workspace, sizeof(s), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    *status = s;
+    if (cudaMemset(workspace, 0, sizeof(s)) != cudaSuccess) return MMN_ERR_CUDA;
+    return MMN_OK;
+}
+
+}  // extern "C"

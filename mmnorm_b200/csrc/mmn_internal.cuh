@@ -1,0 +1,137 @@
+// mmn_internal.cuh -- shared device helpers for the sm_100a backprojection kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mmnorm_b200.h"
+
+namespace mmn {
+
+constexpr double kC = 2.99792458e8;  // imaging_gpu.cu:3
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr int kBlockF = 32;          // samples per re-anchored block
+constexpr size_t kStatusBytes = 256; // workspace header holding the status word
+
+// One virtual antenna, prepared once per call (64 bytes, 16-byte aligned so a chunk
+// of records moves with one bulk copy).
+struct __align__(16) AntRec {
+    double tx[3];   // TX position (plus the optional per-antenna offset)
+    double rx[3];   // RX position = TX + rx_offsets[i % R]
+    float virt[3];  // TX + rx_offset/2 in float32, the vote anchor (surface_normal_est.cu:128-130)
+    float pad;
+};
+static_assert(sizeof(AntRec) == 64, "AntRec must be 64 bytes");
+
+// ---------------------------------------------------------------------------------
+// exp(i*phi) for an FP64 phase of any practical magnitude.
+// The phase is reduced in FP64 to r = phi - n*pi/2 with n = rint(phi*2/pi) (the
+// 1.5*2^52 rounding constant leaves n in the low mantissa bits), then sin and cos of
+// r in [-pi/4, pi/4] are evaluated in FP32 from their Taylor series (terms through
+// r^9 and r^10: truncation below 2e-9), and rotated by n quarter turns.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ float2 cis_fp64_phase(double phi) {
+    const double kTwoOverPi = 0.636619772367581343075535053490057448;
+    const double kPiOver2 = 1.570796326794896619231321691639751442;
+    const double kRound = 6755399441055744.0;  // 1.5 * 2^52
+    double t = fma(phi, kTwoOverPi, kRound);
+    int q = __double2loint(t);
+    double n = t - kRound;
+    float x = (float)fma(-n, kPiOver2, phi);
+    float x2 = x * x;
+    // sin: x - x^3/3! + x^5/5! - x^7/7! + x^9/9!
+    float s = fmaf(x2, 2.75573192239858906526e-6f, -1.98412698412698412698e-4f);
+    s = fmaf(x2, s, 8.33333333333333333333e-3f);
+    s = fmaf(x2, s, -1.66666666666666666667e-1f);
+    s = fmaf(x2 * x, s, x);
+    // cos: 1 - x^2/2! + x^4/4! - x^6/6! + x^8/8! - x^10/10!
+    float c = fmaf(x2, -2.75573192239858906526e-7f, 2.48015873015873015873e-5f);
+    c = fmaf(x2, c, -1.38888888888888888889e-3f);
+    c = fmaf(x2, c, 4.16666666666666666667e-2f);
+    c = fmaf(x2, c, -0.5f);
+    c = fmaf(x2, c, 1.0f);
+    float sr = (q & 1) ? c : s;
+    float cr = (q & 1) ? -s : c;
+    if (q & 2) {
+        sr = -sr;
+        cr = -cr;
+    }
+    return make_float2(cr, sr);
+}
+
+// FP64 round-trip distance TX -> v -> RX.  `mono` (all RX offsets zero) reuses the
+// forward leg for the return leg, which is bit-identical to computing it again.
+__device__ __forceinline__ double range_fp64(double vx, double vy, double vz,
+                                             const AntRec &a, bool mono, double ti) {
+    double dx = vx - a.tx[0], dy = vy - a.tx[1], dz = vz - a.tx[2];
+    double f = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+    double d;
+    if (mono) {
+        d = f + f;
+    } else {
+        double bx = vx - a.rx[0], by = vy - a.rx[1], bz = vz - a.rx[2];
+        d = f + sqrt(fma(bx, bx, fma(by, by, bz * bz)));
+    }
+    return d + ti;
+}
+
+// ---------------------------------------------------------------- status / errors
+__device__ __forceinline__ void set_status(int32_t *status, int32_t code) {
+    if (status) atomicCAS(status, 0, code);
+}
+
+// ----------------------------------------------------------- mbarrier + bulk copy
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Bulk (non-tensor) TMA copy global -> shared, completion counted on `bar`.
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase.  Each try_wait suspends for a hardware-defined
+// interval; after kMaxPolls unsuccessful polls (well beyond any legitimate copy) the
+// wait gives up, records MMN_ERR_TIMEOUT and returns false.
+constexpr uint32_t kMaxPolls = 1u << 24;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  int32_t *status) {
+    for (uint32_t i = 0; i < kMaxPolls; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    set_status(status, MMN_ERR_TIMEOUT);
+    return false;
+}
+
+}  // namespace mmn

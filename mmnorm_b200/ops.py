@@ -1,0 +1,170 @@
+"""Device-resident tensor API over the C ABI (include/mmnorm_b200.h).
+
+All inputs are CUDA tensors; calls are asynchronous on the current torch stream.
+PyTorch provides device memory and streams only -- every computation is one of the
+library's sm_100a kernels, reached through ctypes.
+
+    image, vote = backproject(x, y, z, antenna_locs, rx_offsets, meas, wavelength, slope)
+    normals, mask = surface_normals(image, vote, filter_percent=0.05)
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+C = 2.99792458e8
+
+
+def _vp(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _need(t, name, dtype, device, shape=None):
+    if not isinstance(t, torch.Tensor):
+        raise TypeError("%s must be a torch.Tensor" % name)
+    if t.device != device:
+        raise ValueError("%s is on %s, expected %s" % (name, t.device, device))
+    if t.dtype != dtype:
+        raise TypeError("%s must be %s, got %s" % (name, dtype, t.dtype))
+    if not t.is_contiguous():
+        raise ValueError("%s must be contiguous" % name)
+    if shape is not None and tuple(t.shape) != tuple(shape):
+        raise ValueError("%s must have shape %s, got %s" % (name, shape, tuple(t.shape)))
+    return t
+
+
+def make_problem(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
+                 fft_spacing=0.0, is_ti_radar=False, pos_offsets=None):
+    """Validated ``mmn_problem`` for device tensors (meas: complex64 [A, F])."""
+    dev = meas.device
+    if dev.type != "cuda":
+        raise ValueError("mmnorm_b200 runs on CUDA tensors only (got %s)" % dev)
+    f32 = torch.float32
+    _need(x_locs, "x_locs", f32, dev)
+    _need(y_locs, "y_locs", f32, dev)
+    _need(z_locs, "z_locs", f32, dev)
+    _need(meas, "meas", torch.complex64, dev)
+    if meas.dim() != 2:
+        raise ValueError("meas must be [num_antennas, num_samples]")
+    A, F = meas.shape
+    _need(antenna_locs, "antenna_locs", f32, dev, (A, 3))
+    if rx_offsets.dim() != 2 or rx_offsets.shape[1] != 3:
+        raise ValueError("rx_offsets must be [R, 3]")
+    _need(rx_offsets, "rx_offsets", f32, dev)
+    if pos_offsets is not None:
+        _need(pos_offsets, "pos_offsets", f32, dev, (A, 3))
+    p = _lib.MmnProblem()
+    p.num_x, p.num_y, p.num_z = x_locs.numel(), y_locs.numel(), z_locs.numel()
+    p.x_locs, p.y_locs, p.z_locs = x_locs.data_ptr(), y_locs.data_ptr(), z_locs.data_ptr()
+    p.num_antennas = A
+    p.num_rx = rx_offsets.shape[0]
+    p.antenna_locs = antenna_locs.data_ptr() if A else 0
+    p.rx_offsets = rx_offsets.data_ptr()
+    p.pos_offsets = pos_offsets.data_ptr() if pos_offsets is not None else 0
+    p.num_samples = F
+    p.meas = meas.data_ptr() if A else 0
+    p.wavelength = float(wavelength)
+    p.slope = float(slope)
+    p.fft_spacing = float(fft_spacing)
+    p.is_ti_radar = int(bool(is_ti_radar))
+    return p
+
+
+def workspace_bytes(problem, mode="mixed"):
+    n = _lib.load().mmn_workspace_bytes(ctypes.byref(problem), _lib.MODES[mode], 1)
+    if n == 0:
+        raise _lib.MmnError(_lib.MMN_ERR_INVALID_ARGUMENT, "mmn_workspace_bytes")
+    return n
+
+
+def plan_info(problem, mode="mixed"):
+    vals = [ctypes.c_int32() for _ in range(5)]
+    rc = _lib.load().mmn_plan_info(ctypes.byref(problem), _lib.MODES[mode],
+                                   *[ctypes.byref(v) for v in vals])
+    _lib.check(rc, "mmn_plan_info")
+    keys = ("tiles", "splits", "antennas_per_stage", "threads", "voxels_per_thread")
+    return {k: v.value for k, v in zip(keys, vals)}
+
+
+def backproject(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope, *,
+                mode="mixed", fft_spacing=0.0, is_ti_radar=False, pos_offsets=None,
+                want_vote=True, workspace=None):
+    """Fused backprojection + vote.
+
+    Returns ``image`` complex64 [NX, NY, NZ] (raw sum over virtual antennas and samples,
+    not normalised) and ``vote`` complex64 [3, NX, NY, NZ] (or None).
+    ``mode``: 'mixed' (FP64 range/wrap + FP32 recurrence), 'plain' (FP32 sincos per
+    sample) or 'interp' (reference interpolated mode; ``meas`` holds range-FFT bins).
+    """
+    p = make_problem(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength,
+                     slope, fft_spacing, is_ti_radar, pos_offsets)
+    dev = meas.device
+    nx, ny, nz = p.num_x, p.num_y, p.num_z
+    V = nx * ny * nz
+    image = torch.empty(V, dtype=torch.complex64, device=dev)
+    vote = torch.empty((3, V), dtype=torch.complex64, device=dev) if want_vote else None
+    lib = _lib.load()
+    nbytes = workspace_bytes(p, mode)
+    if workspace is None or workspace.numel() < nbytes:
+        workspace = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    rc = lib.mmn_backproject(ctypes.byref(p), _lib.MODES[mode], _vp(image), _vp(vote),
+                             _vp(workspace), workspace.numel(), _stream(dev))
+    _lib.check(rc, "mmn_backproject")
+    return image.view(nx, ny, nz), (vote.view(3, nx, ny, nz) if vote is not None else None)
+
+
+def surface_normals(image, vote, filter_percent=0.05, want_raw=False):
+    """Unit normals float32 [..., 3] (NaN outside the mask), the bool mask, and
+    optionally the raw (un-normalised) normal Re(conj(I) W)/|I|."""
+    dev = image.device
+    shape = tuple(image.shape)
+    V = image.numel()
+    img = image.reshape(V)
+    w = vote.reshape(3, V)
+    _need(img, "image", torch.complex64, dev)
+    _need(w, "vote", torch.complex64, dev)
+    normals = torch.empty((V, 3), dtype=torch.float32, device=dev)
+    mask = torch.empty(V, dtype=torch.uint8, device=dev)
+    raw = torch.empty((V, 3), dtype=torch.float32, device=dev) if want_raw else None
+    lib = _lib.load()
+    nbytes = lib.mmn_normals_workspace_bytes(V)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    rc = lib.mmn_normals(V, _vp(img), _vp(w), float(filter_percent), _vp(normals), _vp(mask),
+                         _vp(raw), _vp(ws), nbytes, _stream(dev))
+    _lib.check(rc, "mmn_normals")
+    out = (normals.view(*shape, 3), mask.view(shape).bool())
+    if want_raw:
+        out = out + (raw.view(*shape, 3),)
+    return out
+
+
+def read_status(workspace):
+    """Synchronise and return (and clear) the in-kernel status word of a workspace."""
+    st = ctypes.c_int32(0)
+    rc = _lib.load().mmn_read_status(_vp(workspace), ctypes.byref(st),
+                                     _stream(workspace.device))
+    _lib.check(rc, "mmn_read_status")
+    return st.value
+
+
+def variants(mode="mixed"):
+    lib = _lib.load()
+    m = _lib.MODES[mode]
+    out = []
+    for i in range(lib.mmn_num_variants(m)):
+        t, nt = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(lib.mmn_variant_info(m, i, ctypes.byref(t), ctypes.byref(nt)),
+                   "mmn_variant_info")
+        out.append({"index": i, "voxels_per_thread": t.value, "threads": nt.value})
+    return out
+
+
+def set_variant(mode, index):
+    _lib.check(_lib.load().mmn_set_variant(_lib.MODES[mode], int(index)), "mmn_set_variant")

@@ -1,0 +1,59 @@
+"""The C-ABI library loads and exports every entry point include/mmnorm_b200.h declares;
+argument validation paths that need no device return the documented codes.  CPU only:
+no compute call is made."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "mmnorm_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(mmn_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    for must in ("mmn_backproject", "mmn_normals", "mmn_cuda_image", "mmn_cuda_sn_est",
+                 "mmn_workspace_bytes", "mmn_read_status"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from mmnorm_b200 import _lib
+    h = _lib.load()
+    for name in _declared():
+        assert hasattr(h, name), name
+    bound = {n for n, _, _ in _lib.SIGNATURES}
+    assert set(_declared()) <= bound, set(_declared()) - bound
+
+
+def test_version_and_validation_without_device():
+    from mmnorm_b200 import _lib
+    h = _lib.load()
+    assert h.mmn_version().startswith(b"mmnorm_b200")
+    assert h.mmn_backproject(None, 0, None, None, None, 0, None) == _lib.MMN_ERR_NULL_POINTER
+    p = _lib.MmnProblem()
+    p.num_x = 0
+    assert h.mmn_workspace_bytes(ctypes.byref(p), 0, 1) == 0
+    p.num_x = p.num_y = p.num_z = 4
+    p.num_rx = 1
+    p.num_samples = 8
+    p.wavelength = 3.9e-3
+    assert h.mmn_backproject(ctypes.byref(p), 9, None, None, None, 0, None) == \
+        _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_backproject(ctypes.byref(p), 0, None, None, None, 0, None) == \
+        _lib.MMN_ERR_NULL_POINTER
+    assert h.mmn_normals(0, None, None, 0.05, None, None, None, None, 0, None) == \
+        _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_set_variant(7, 0) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_num_variants(_lib.MODE_MIXED) >= 1
+    assert h.mmn_num_variants(_lib.MODE_PLAIN) >= 1
+
+
+def test_library_is_sm100a_only_build():
+    """The build recipe targets exactly sm_100a."""
+    from mmnorm_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
