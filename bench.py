@@ -45,6 +45,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU seconds of the bounded reference/CPU sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--aperture", type=int, default=128,
+                    help="aperture side (antennas); smaller values make a profiling case "
+                         "with the same kernel and voxel grid (the default is the workload)")
     return ap.parse_args()
 
 
@@ -103,9 +107,18 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- the scene
-def load_scene(device):
+def load_scene(device, aperture=128):
     from mmnorm_b200 import scenes
-    return scenes.config1(sign=-1, device=device)
+    sc = scenes.config1(sign=-1, device=device)
+    if aperture != 128:
+        # profiling case: the central aperture x aperture antennas of the same scene
+        n0 = (128 - aperture) // 2
+        idx = (np.arange(n0, n0 + aperture)[:, None] * 128 +
+               np.arange(n0, n0 + aperture)[None, :]).ravel()
+        sc.antenna_locs = np.ascontiguousarray(sc.antenna_locs[idx])
+        sc.meas = np.ascontiguousarray(sc.meas[idx])
+        sc.name = sc.name.replace("ap128", "ap%d" % aperture)
+    return sc
 
 
 def cpu_sample_axes(sc, n_voxels_target, cores):
@@ -204,7 +217,7 @@ def ours_arm(args):
     import torch
     import torch.distributed as dist
 
-    from mmnorm_b200 import _lib, ops
+    from mmnorm_b200 import _lib, autotune, ops
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -218,7 +231,7 @@ def ours_arm(args):
     lib = _lib.load()
     _lib.check(lib.mmn_check_device(local), "mmn_check_device")
 
-    sc = load_scene(dev)
+    sc = load_scene(dev, args.aperture)
     A, F = sc.meas.shape
     V = sc.num_voxels
     updates = V * A * F
@@ -226,6 +239,8 @@ def ours_arm(args):
     xs, ys, zs = t(sc.x_locs), t(sc.y_locs), t(sc.z_locs)
     ant, rxo = t(sc.antenna_locs), t(np.zeros((1, 3), np.float32))
     meas = t(sc.meas)
+    tuned = autotune.tune(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope, mode="mixed")
+    variant = ops.variants("mixed")[tuned["best"]]
     prob = ops.make_problem(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope)
     ws = torch.empty(ops.workspace_bytes(prob, "mixed"), dtype=torch.uint8, device=dev)
     plan = ops.plan_info(prob, "mixed")
@@ -293,6 +308,8 @@ def ours_arm(args):
     out = {}
     if rank == 0 and world == 1 and args.plain_steps > 0:
         # plain FP32 sincos-per-sample form on the same workload
+        ptuned = autotune.tune(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope,
+                               mode="plain", max_antennas=256)
         step("plain")
         pe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.plain_steps)]
@@ -307,12 +324,13 @@ def ours_arm(args):
         pval = updates / (pms * 1e-3) / 1e9
         out["plain"] = {"value": pval, "unit": UNIT, "ms_per_step": pms,
                         "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in pe),
-                        "mixed_over_plain": value / pval}
+                        "mixed_over_plain": value / pval,
+                        "variant": ops.variants("plain")[ptuned["best"]]["name"]}
 
     # end to end through the public API: pinned host inputs -> device -> image + normals
     # -> pinned host outputs, every step
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         h_meas = torch.empty(meas.shape, dtype=meas.dtype, pin_memory=True)
         h_meas.copy_(torch.as_tensor(sc.meas))
         h_ant = torch.as_tensor(sc.antenna_locs).pin_memory()
@@ -381,11 +399,12 @@ def ours_arm(args):
                        "voxels": V, "antennas": A, "freqs": F,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "flushed before every step (256 MB write)",
-                       "plan": plan},
+                       "plan": plan, "variant": variant["name"],
+                       "autotune_ms": tuned["times_ms"]},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": _read_traffic(),
-                         "kernel": "bp_fwd_kernel<4,128,mixed>",
+                         "kernel": "bp_fwd_kernel " + variant["name"],
                          "flops_per_update": 8,
                          "peak_source": "FP32 FFMA probe (mmn_fp32_peak_probe) timed in this "
                                         "run; MEASURED_PEAKS.json has no FP32 figure",

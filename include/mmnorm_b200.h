@@ -80,6 +80,7 @@ size_t mmn_workspace_bytes(const mmn_problem *p, int32_t mode, int32_t want_vote
 int mmn_num_variants(int32_t mode);
 int mmn_variant_info(int32_t mode, int32_t idx, int32_t *voxels_per_thread, int32_t *threads);
 int mmn_set_variant(int32_t mode, int32_t idx);
+const char *mmn_variant_name(int32_t mode, int32_t idx); /* NULL for a bad index */
 
 /* The decomposition mmn_backproject will use for `p`: voxel tiles, antenna splits,
  * antennas per shared-memory stage, threads per CTA, voxels per thread. */

@@ -74,6 +74,7 @@ SIGNATURES = [
     ("mmn_num_variants", _I, [_I32]),
     ("mmn_variant_info", _I, [_I32, _I32, _I32P, _I32P]),
     ("mmn_set_variant", _I, [_I32, _I32]),
+    ("mmn_variant_name", ctypes.c_char_p, [_I32, _I32]),
     ("mmn_plan_info", _I, [_PROB, _I32, _I32P, _I32P, _I32P, _I32P, _I32P]),
     ("mmn_backproject", _I, [_PROB, _I32, _P, _P, _P, _SZ, _P]),
     ("mmn_normals_workspace_bytes", _SZ, [ctypes.c_int64]),

@@ -1,0 +1,84 @@
+"""Autotuner for the forward kernels' launch shape (voxels per thread x threads per CTA;
+the antenna stage size and the antenna split follow from the plan).
+
+Each candidate variant is timed with CUDA events on a reduced copy of the problem: the
+same voxel grid and sample count with at most ``max_antennas`` antennas, which keeps the
+per-update work of every variant identical to the full problem while bounding the tuning
+time.  The winner is cached per (device, mode, padded sample count, voxel-count bucket)
+in memory and, optionally, in a JSON file.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import torch
+
+from . import ops
+
+_cache: dict = {}
+
+
+def _key(device, mode, nvox, nsamples):
+    name = torch.cuda.get_device_name(device)
+    fp = (nsamples + 31) // 32 * 32
+    vb = int(math.log2(max(1, nvox)))
+    return "%s|%s|F%d|V2^%d" % (name, mode, fp, vb)
+
+
+def load_cache(path):
+    if path and os.path.exists(path):
+        with open(path) as f:
+            _cache.update(json.load(f))
+
+
+def save_cache(path):
+    if path:
+        with open(path, "w") as f:
+            json.dump(_cache, f, indent=1, sort_keys=True)
+
+
+def tune(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope, *,
+         mode="mixed", max_antennas=1024, repeats=2, apply=True, verbose=False):
+    """Times every variant of ``mode`` and (if ``apply``) selects the fastest.
+
+    Returns {"key", "best", "times_ms": {variant index: ms}}."""
+    dev = meas.device
+    nvox = x_locs.numel() * y_locs.numel() * z_locs.numel()
+    key = _key(dev, mode, nvox, meas.shape[1])
+    if key in _cache:
+        res = _cache[key]
+        if apply:
+            ops.set_variant(mode, res["best"])
+        return res
+    A = meas.shape[0]
+    n = min(A, max_antennas)
+    sel = torch.linspace(0, A - 1, n, device=dev).round().long() if n < A else None
+    ant = antenna_locs[sel].contiguous() if sel is not None else antenna_locs
+    m = meas[sel].contiguous() if sel is not None else meas
+    times = {}
+    stream = torch.cuda.current_stream(dev)
+    for v in ops.variants(mode):
+        idx = v["index"]
+        ops.set_variant(mode, idx)
+        ops.backproject(x_locs, y_locs, z_locs, ant, rx_offsets, m, wavelength, slope, mode=mode)
+        best = float("inf")
+        for _ in range(repeats):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ops.backproject(x_locs, y_locs, z_locs, ant, rx_offsets, m, wavelength, slope,
+                            mode=mode)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            best = min(best, e0.elapsed_time(e1))
+        times[idx] = best
+        if verbose:
+            print("autotune %s variant %d (%s): %.3f ms" % (mode, idx, v, best))
+    best_idx = min(times, key=times.get)
+    res = {"key": key, "best": best_idx, "times_ms": {str(k): t for k, t in times.items()},
+           "variants": ops.variants(mode), "antennas_timed": n}
+    _cache[key] = res
+    ops.set_variant(mode, best_idx if apply else 0)
+    return res

@@ -14,11 +14,15 @@
 //
 // MIXED form (default).  Per (voxel, antenna): d in FP64; the sample sum is split
 // into blocks of 32 samples, each evaluated by Horner's rule in FP32,
-//     h_b = sum_{t<32} m[i, 32b+t] * z^t,   z = exp(-j d kappa_step)   (4 FFMA / sample)
+//     h_b = sum_{t<32} m[i, 32b+t] * z^t,   z = exp(-j d kappa_step)   (4 FMA / sample)
 // i.e. the rotation recurrence is applied to the running partial sum instead of to a
 // separate phasor, and every block is re-anchored with the exact FP64-wrapped phase
 //     c_i += exp(-j d kappa_{32b}) * h_b.
-// The per-sample work is one complex multiply-add (4 FFMA), no SFU.
+// The per-sample work is one complex multiply-add, no SFU.  The default kernel runs a
+// thread's voxels in PAIRS with Blackwell's packed FFMA2 (two FP32 FMAs per issue
+// slot): each Horner step of a voxel pair is 4 FFMA2, reading the sample from a
+// (re, re, im, im) record so one broadcast 16-byte shared load feeds both halves.
+// The scalar-FFMA version of the same kernel is kept as an autotuner variant.
 //
 // PLAIN form.  FP32 distance and FP32 phase -d*kappa_j with one sincosf per sample,
 // then a complex multiply-add -- the straightforward FP32 kernel.
@@ -26,92 +30,126 @@
 // Work item = (voxel tile, antenna split).  A CTA of NT threads owns NT*T voxels (T
 // per thread, strided by NT so stores coalesce).  Antenna records and measurement
 // rows stream through a double-buffered shared-memory stage filled by one elected
-// thread with bulk TMA copies (cp.async.bulk) completing on an mbarrier; every
-// thread reads the samples as broadcast float4 loads (two complex samples).  With
-// one split per tile the CTA writes the final image/vote; otherwise it writes an
-// 8-float partial per voxel that bp_reduce_partials sums in split order
-// (deterministic).
+// thread with bulk TMA copies (cp.async.bulk) completing on an mbarrier.  With one
+// split per tile the CTA writes the final image/vote; otherwise it writes an 8-float
+// partial per voxel that bp_reduce_partials sums in split order (deterministic).
 #include "bp_kernels.cuh"
 
 namespace mmn {
 
-template <int T>
-__device__ __forceinline__ void horner_step(float (&hr)[T], float (&hi)[T],
-                                            const float (&zr)[T], const float (&zi)[T],
-                                            const float (&nzi)[T], float mr, float mi) {
-#pragma unroll
-    for (int k = 0; k < T; ++k) {
-        float a = fmaf(hr[k], zr[k], mr);
-        float b = fmaf(hr[k], zi[k], mi);
-        hr[k] = fmaf(hi[k], nzi[k], a);
-        hi[k] = fmaf(hi[k], zr[k], b);
+namespace {
+
+// ----------------------------------------------------------- shared-memory stage
+struct Stage {
+    uint64_t *bars;
+    unsigned char *base;
+    size_t stage_bytes;
+    int nas;
+    int esz;  // bytes per sample in shared memory (8: (re, im); 16: (re, re, im, im))
+    int fp;
+
+    __device__ void issue(const FwdParams &p, int c, int a_begin, int a_end) const {
+        const int s = c & 1;
+        const int a0 = a_begin + c * nas;
+        const int na = min(nas, a_end - a0);
+        unsigned char *st = base + s * stage_bytes;
+        const uint32_t ant_bytes = (uint32_t)(na * sizeof(AntRec));
+        const uint32_t meas_bytes = (uint32_t)((size_t)na * fp * esz);
+        mbar_arrive_expect_tx(&bars[s], ant_bytes + meas_bytes);
+        bulk_g2s(st, p.ant + a0, ant_bytes, &bars[s]);
+        bulk_g2s(st + (size_t)nas * sizeof(AntRec),
+                 static_cast<const unsigned char *>(p.meas) + (size_t)a0 * fp * esz,
+                 meas_bytes, &bars[s]);
+    }
+    __device__ const AntRec *ants(int s) const {
+        return reinterpret_cast<const AntRec *>(base + s * stage_bytes);
+    }
+    __device__ const unsigned char *meas(int s) const {
+        return base + s * stage_bytes + (size_t)nas * sizeof(AntRec);
+    }
+};
+
+__device__ __forceinline__ void decode_voxel(const FwdParams &p, int64_t rel, float &x,
+                                             float &y, float &z) {
+    const int64_t v = rel < p.vox_count ? p.vox_start + rel : p.vox_start;
+    const int64_t nyz = (int64_t)p.ny * p.nz;
+    const int ix = (int)(v / nyz);
+    const int64_t rem = v - (int64_t)ix * nyz;
+    const int iy = (int)(rem / p.nz);
+    const int iz = (int)(rem - (int64_t)iy * p.nz);
+    x = __ldg(p.x_locs + ix);
+    y = __ldg(p.y_locs + iy);
+    z = __ldg(p.z_locs + iz);
+}
+
+__device__ __forceinline__ void store_voxel(const FwdParams &p, int split, int64_t rel,
+                                            const float (&a)[8]) {
+    if (rel >= p.vox_count) return;
+    const int64_t v = p.vox_start + rel;
+    if (p.num_splits == 1) {
+        if (p.image) p.image[v] = make_float2(a[0], a[1]);
+        if (p.out_r) {
+            p.out_r[v] = a[0];
+            p.out_i[v] = a[1];
+        }
+        if (p.vote) {
+            p.vote[v] = make_float2(a[2], a[3]);
+            p.vote[p.nvox + v] = make_float2(a[4], a[5]);
+            p.vote[2 * p.nvox + v] = make_float2(a[6], a[7]);
+        }
+    } else {
+        float4 *dst = p.partial + 2 * ((size_t)split * p.vox_count + rel);
+        dst[0] = make_float4(a[0], a[1], a[2], a[3]);
+        dst[1] = make_float4(a[4], a[5], a[6], a[7]);
     }
 }
 
-template <int T, int NT, bool PLAIN>
+}  // namespace
+
+// Kernel forms
+constexpr int kFormMixedPair = 0;    // FFMA2 voxel pairs, (re,re,im,im) samples
+constexpr int kFormMixedScalar = 1;  // scalar FFMA, (re,im) samples
+constexpr int kFormPlain = 2;        // FP32 sincosf per sample, (re,im) samples
+
+template <int T, int NT, int FORM>
 __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
+    static_assert(FORM != kFormMixedPair || T % 2 == 0, "pair form needs an even T");
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    Stage st;
+    st.bars = reinterpret_cast<uint64_t *>(smem);
+    st.base = smem + 128;
+    st.nas = p.ant_per_stage;
+    st.esz = FORM == kFormMixedPair ? 16 : 8;
+    st.fp = p.fp;
+    st.stage_bytes = (size_t)st.nas * sizeof(AntRec) + (size_t)st.nas * st.fp * st.esz;
+    float *kappa_tab = reinterpret_cast<float *>(st.base + 2 * st.stage_bytes);  // PLAIN only
     const int fp = p.fp;
-    const int nas = p.ant_per_stage;
-    const size_t stage_bytes = (size_t)nas * sizeof(AntRec) + (size_t)nas * fp * sizeof(float2);
-    unsigned char *stage_base = smem + 128;
-    float *kappa_tab = reinterpret_cast<float *>(stage_base + 2 * stage_bytes);  // PLAIN only
 
     const int tile = blockIdx.x % p.num_tiles;
     const int split = blockIdx.x / p.num_tiles;
     const int a_begin = split * p.ant_per_split;
     const int a_end = min(p.num_ant, a_begin + p.ant_per_split);
-    const int n_chunks = a_end > a_begin ? (a_end - a_begin + nas - 1) / nas : 0;
+    const int n_chunks = a_end > a_begin ? (a_end - a_begin + st.nas - 1) / st.nas : 0;
 
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        mbar_init(&st.bars[0], 1);
+        mbar_init(&st.bars[1], 1);
         fence_mbar_init();
     }
-    if (PLAIN) {
+    if constexpr (FORM == kFormPlain) {
         for (int j = threadIdx.x; j < fp; j += NT)
             kappa_tab[j] = (float)fma((double)j, p.kd, p.k0);
     }
     __syncthreads();
-
-    auto issue = [&](int c) {
-        const int s = c & 1;
-        const int a0 = a_begin + c * nas;
-        const int na = min(nas, a_end - a0);
-        unsigned char *st = stage_base + s * stage_bytes;
-        const uint32_t ant_bytes = (uint32_t)(na * sizeof(AntRec));
-        const uint32_t meas_bytes = (uint32_t)((size_t)na * fp * sizeof(float2));
-        mbar_arrive_expect_tx(&bars[s], ant_bytes + meas_bytes);
-        bulk_g2s(st, p.ant + a0, ant_bytes, &bars[s]);
-        bulk_g2s(st + (size_t)nas * sizeof(AntRec), p.meas + (size_t)a0 * fp, meas_bytes,
-                 &bars[s]);
-    };
     if (threadIdx.x == 0) {
-        if (n_chunks > 0) issue(0);
-        if (n_chunks > 1) issue(1);
+        if (n_chunks > 0) st.issue(p, 0, a_begin, a_end);
+        if (n_chunks > 1) st.issue(p, 1, a_begin, a_end);
     }
 
-    // voxels of this thread: rel = tile*NT*T + tid + k*NT, voxel = vox_start + rel
     const int64_t rbase = (int64_t)tile * (NT * T) + threadIdx.x;
     float vx[T], vy[T], vz[T];
-    double vxd[T], vyd[T], vzd[T];
 #pragma unroll
-    for (int k = 0; k < T; ++k) {
-        const int64_t rel = rbase + (int64_t)k * NT;
-        const int64_t v = rel < p.vox_count ? p.vox_start + rel : p.vox_start;
-        const int64_t nyz = (int64_t)p.ny * p.nz;
-        const int ix = (int)(v / nyz);
-        const int64_t rem = v - (int64_t)ix * nyz;
-        const int iy = (int)(rem / p.nz);
-        const int iz = (int)(rem - (int64_t)iy * p.nz);
-        vx[k] = __ldg(p.x_locs + ix);
-        vy[k] = __ldg(p.y_locs + iy);
-        vz[k] = __ldg(p.z_locs + iz);
-        vxd[k] = vx[k];
-        vyd[k] = vy[k];
-        vzd[k] = vz[k];
-    }
+    for (int k = 0; k < T; ++k) decode_voxel(p, rbase + (int64_t)k * NT, vx[k], vy[k], vz[k]);
     float acc[T][8];
 #pragma unroll
     for (int k = 0; k < T; ++k)
@@ -123,30 +161,77 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
 
     for (int c = 0; c < n_chunks; ++c) {
         const int s = c & 1;
-        bool ok = mbar_wait_bounded(&bars[s], (uint32_t)((c >> 1) & 1), p.status);
+        bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
         if (!__syncthreads_and(ok)) return;
-        const AntRec *ants = reinterpret_cast<const AntRec *>(stage_base + s * stage_bytes);
-        const float4 *meas4 = reinterpret_cast<const float4 *>(
-            stage_base + s * stage_bytes + (size_t)nas * sizeof(AntRec));
-        const int na = min(nas, a_end - (a_begin + c * nas));
+        const AntRec *ants = st.ants(s);
+        const unsigned char *mstage = st.meas(s);
+        const int na = min(st.nas, a_end - (a_begin + c * st.nas));
 
         for (int a = 0; a < na; ++a) {
             const AntRec &ar = ants[a];
-            const float4 *m4 = meas4 + (size_t)a * (fp / 2);
             float cr[T], ci[T];
+            if constexpr (FORM == kFormMixedPair) {
+                constexpr int P = T / 2;
+                const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * fp;
+                double d[T];
+                float2 zr[P], zi[P], nzi[P], c2r[P], c2i[P];
 #pragma unroll
-            for (int k = 0; k < T; ++k) cr[k] = ci[k] = 0.f;
-
-            if (!PLAIN) {
+                for (int k = 0; k < T; ++k)
+                    d[k] = range_fp64((double)vx[k], (double)vy[k], (double)vz[k], ar, mono, p.ti);
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    cis_fp64_phase_pair(-d[2 * q] * p.kd, -d[2 * q + 1] * p.kd, zr[q], zi[q], nzi[q]);
+                    c2r[q] = c2i[q] = make_float2(0.f, 0.f);
+                }
+                for (int b = 0; b < nblk; ++b) {
+                    const float4 *mb = m4 + b * kBlockF;
+                    float2 hr[P], hi[P];
+                    const float4 top = mb[kBlockF - 1];
+#pragma unroll
+                    for (int q = 0; q < P; ++q) {
+                        hr[q] = make_float2(top.x, top.y);
+                        hi[q] = make_float2(top.z, top.w);
+                    }
+#pragma unroll
+                    for (int t = kBlockF - 2; t >= 0; --t) {
+                        const float4 mm = mb[t];
+                        const float2 mr = make_float2(mm.x, mm.y), mi = make_float2(mm.z, mm.w);
+#pragma unroll
+                        for (int q = 0; q < P; ++q) {
+                            const float2 u = __ffma2_rn(hr[q], zr[q], mr);
+                            const float2 w = __ffma2_rn(hr[q], zi[q], mi);
+                            hr[q] = __ffma2_rn(hi[q], nzi[q], u);
+                            hi[q] = __ffma2_rn(hi[q], zr[q], w);
+                        }
+                    }
+                    const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
+#pragma unroll
+                    for (int q = 0; q < P; ++q) {
+                        float2 anr, ani, nani;
+                        cis_fp64_phase_pair(-d[2 * q] * kap, -d[2 * q + 1] * kap, anr, ani, nani);
+                        c2r[q] = __ffma2_rn(anr, hr[q], __ffma2_rn(nani, hi[q], c2r[q]));
+                        c2i[q] = __ffma2_rn(anr, hi[q], __ffma2_rn(ani, hr[q], c2i[q]));
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    cr[2 * q] = c2r[q].x;
+                    cr[2 * q + 1] = c2r[q].y;
+                    ci[2 * q] = c2i[q].x;
+                    ci[2 * q + 1] = c2i[q].y;
+                }
+            } else if constexpr (FORM == kFormMixedScalar) {
+                const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
                 double d[T];
                 float zr[T], zi[T], nzi[T];
 #pragma unroll
                 for (int k = 0; k < T; ++k) {
-                    d[k] = range_fp64(vxd[k], vyd[k], vzd[k], ar, mono, p.ti);
-                    float2 z = cis_fp64_phase(-d[k] * p.kd);
+                    d[k] = range_fp64((double)vx[k], (double)vy[k], (double)vz[k], ar, mono, p.ti);
+                    const float2 z = cis_fp64_phase(-d[k] * p.kd);
                     zr[k] = z.x;
                     zi[k] = z.y;
                     nzi[k] = -z.y;
+                    cr[k] = ci[k] = 0.f;
                 }
                 for (int b = 0; b < nblk; ++b) {
                     const float4 *mb = m4 + b * (kBlockF / 2);
@@ -156,13 +241,25 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                     for (int k = 0; k < T; ++k) {
                         hr[k] = top.z;
                         hi[k] = top.w;
+                        const float u = fmaf(hr[k], zr[k], top.x);
+                        const float w = fmaf(hr[k], zi[k], top.y);
+                        hr[k] = fmaf(hi[k], nzi[k], u);
+                        hi[k] = fmaf(hi[k], zr[k], w);
                     }
-                    horner_step<T>(hr, hi, zr, zi, nzi, top.x, top.y);
 #pragma unroll
                     for (int q = kBlockF / 2 - 2; q >= 0; --q) {
                         const float4 mm = mb[q];
-                        horner_step<T>(hr, hi, zr, zi, nzi, mm.z, mm.w);
-                        horner_step<T>(hr, hi, zr, zi, nzi, mm.x, mm.y);
+#pragma unroll
+                        for (int k = 0; k < T; ++k) {
+                            float u = fmaf(hr[k], zr[k], mm.z);
+                            float w = fmaf(hr[k], zi[k], mm.w);
+                            hr[k] = fmaf(hi[k], nzi[k], u);
+                            hi[k] = fmaf(hi[k], zr[k], w);
+                            u = fmaf(hr[k], zr[k], mm.x);
+                            w = fmaf(hr[k], zi[k], mm.y);
+                            hr[k] = fmaf(hi[k], nzi[k], u);
+                            hi[k] = fmaf(hi[k], zr[k], w);
+                        }
                     }
                     const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
 #pragma unroll
@@ -174,6 +271,7 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                 }
             } else {
                 // FP32 distance as the reference computes it (imaging_gpu.cu:67-88)
+                const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
                 float df[T];
                 const float tx = (float)ar.tx[0], ty = (float)ar.tx[1], tz = (float)ar.tx[2];
                 const float ox = (float)(ar.rx[0] - ar.tx[0]), oy = (float)(ar.rx[1] - ar.tx[1]),
@@ -184,6 +282,7 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                     const float f = sqrtf(ax * ax + ay * ay + az * az);
                     const float bx = ax - ox, by = ay - oy, bz = az - oz;
                     df[k] = f + sqrtf(bx * bx + by * by + bz * bz) + (float)p.ti;
+                    cr[k] = ci[k] = 0.f;
                 }
                 const float2 *kap2 = reinterpret_cast<const float2 *>(kappa_tab);
                 for (int b = 0; b < nblk; ++b) {
@@ -220,31 +319,11 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0 && c + 2 < n_chunks) issue(c + 2);
+        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
     }
 
 #pragma unroll
-    for (int k = 0; k < T; ++k) {
-        const int64_t rel = rbase + (int64_t)k * NT;
-        if (rel >= p.vox_count) continue;
-        const int64_t v = p.vox_start + rel;
-        if (p.num_splits == 1) {
-            if (p.image) p.image[v] = make_float2(acc[k][0], acc[k][1]);
-            if (p.out_r) {
-                p.out_r[v] = acc[k][0];
-                p.out_i[v] = acc[k][1];
-            }
-            if (p.vote) {
-                p.vote[v] = make_float2(acc[k][2], acc[k][3]);
-                p.vote[p.nvox + v] = make_float2(acc[k][4], acc[k][5]);
-                p.vote[2 * p.nvox + v] = make_float2(acc[k][6], acc[k][7]);
-            }
-        } else {
-            float4 *dst = p.partial + 2 * ((size_t)split * p.vox_count + rel);
-            dst[0] = make_float4(acc[k][0], acc[k][1], acc[k][2], acc[k][3]);
-            dst[1] = make_float4(acc[k][4], acc[k][5], acc[k][6], acc[k][7]);
-        }
-    }
+    for (int k = 0; k < T; ++k) store_voxel(p, split, rbase + (int64_t)k * NT, acc[k]);
 }
 
 __global__ void bp_reduce_partials(const FwdParams p) {
@@ -272,7 +351,8 @@ __global__ void bp_reduce_partials(const FwdParams p) {
 
 // Builds the 64-byte antenna records: TX (+ optional per-antenna offset), RX = TX +
 // rx_offsets[i % R], and the float32 vote anchor TX + o/2 computed as the reference
-// does (surface_normal_est.cu:128-130).
+// does (surface_normal_est.cu:128-130).  Thread 0 also records whether every RX offset
+// is zero (the forward kernels then reuse the outgoing leg for the return leg).
 __global__ void prep_antennas(const float *__restrict__ ant, const float *__restrict__ rxo,
                               int R, const float *__restrict__ pos_off, int A,
                               AntRec *__restrict__ out, int32_t *__restrict__ mono_flag) {
@@ -302,43 +382,50 @@ __global__ void prep_antennas(const float *__restrict__ ant, const float *__rest
     out[i] = r;
 }
 
-// Copies [A, F] complex64 rows into [A, Fp] rows zero-padded to Fp (Fp % 32 == 0).
-// Zero samples at the top of a Horner block contribute exactly nothing.
-__global__ void pad_meas(const float2 *__restrict__ src, int A, int F, float2 *__restrict__ dst,
-                         int Fp) {
+// Measurement rows [A, F] (complex64, or SoA planes re/im when `im` is non-null) into
+// the shared-memory layout of a kernel form: rows of Fp = roundup(F, 32) samples,
+// zero-padded (zero samples at the top of a Horner block add exactly nothing), each
+// sample either (re, im) (esz 8) or (re, re, im, im) (esz 16).
+__global__ void stage_meas(const float *__restrict__ src, const float *__restrict__ im, int A,
+                           int F, int Fp, int esz, void *__restrict__ dst) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)A * Fp) return;
     const int64_t a = idx / Fp;
     const int j = (int)(idx - a * Fp);
-    dst[idx] = j < F ? src[a * F + j] : make_float2(0.f, 0.f);
-}
-
-// Interleaves SoA measurement planes (the reference's meas_r / meas_i layout,
-// py_image_gpu.py:261-262) into padded complex64 rows.
-__global__ void interleave_pad_meas(const float *__restrict__ re, const float *__restrict__ im,
-                                    int A, int F, float2 *__restrict__ dst, int Fp) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)A * Fp) return;
-    const int64_t a = idx / Fp;
-    const int j = (int)(idx - a * Fp);
-    dst[idx] = j < F ? make_float2(re[a * F + j], im[a * F + j]) : make_float2(0.f, 0.f);
+    float re = 0.f, ig = 0.f;
+    if (j < F) {
+        if (im) {
+            re = src[a * F + j];
+            ig = im[a * F + j];
+        } else {
+            const float2 m = reinterpret_cast<const float2 *>(src)[a * F + j];
+            re = m.x;
+            ig = m.y;
+        }
+    }
+    if (esz == 16)
+        reinterpret_cast<float4 *>(dst)[idx] = make_float4(re, re, ig, ig);
+    else
+        reinterpret_cast<float2 *>(dst)[idx] = make_float2(re, ig);
 }
 
 // ------------------------------------------------------------------ instantiations
-template <int T, int NT, bool PLAIN>
+template <int T, int NT, int FORM>
 static const void *fwd_ptr() {
-    return reinterpret_cast<const void *>(&bp_fwd_kernel<T, NT, PLAIN>);
+    return reinterpret_cast<const void *>(&bp_fwd_kernel<T, NT, FORM>);
 }
 
 const FwdVariant *fwd_variants(int *count) {
+    // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
-        {4, 128, false, fwd_ptr<4, 128, false>()},
-        {2, 128, false, fwd_ptr<2, 128, false>()},
-        {4, 256, false, fwd_ptr<4, 256, false>()},
-        {2, 256, false, fwd_ptr<2, 256, false>()},
-        {2, 128, true, fwd_ptr<2, 128, true>()},
-        {1, 128, true, fwd_ptr<1, 128, true>()},
-        {2, 256, true, fwd_ptr<2, 256, true>()},
+        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair>(), "mixed_ffma2_t4_n128"},
+        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPair>(), "mixed_ffma2_t2_n128"},
+        {4, 256, false, 16, fwd_ptr<4, 256, kFormMixedPair>(), "mixed_ffma2_t4_n256"},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair>(), "mixed_ffma2_t2_n256"},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedScalar>(), "mixed_ffma_t4_n128"},
+        {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128"},
+        {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128"},
+        {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256"},
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
     return v;
@@ -365,19 +452,11 @@ cudaError_t launch_prep_antennas(const float *ant, const float *rxo, int R, cons
     return cudaGetLastError();
 }
 
-cudaError_t launch_pad_meas(const float2 *src, int A, int F, float2 *dst, int Fp,
-                            cudaStream_t stream) {
+cudaError_t launch_stage_meas(const float *src, const float *im, int A, int F, int Fp, int esz,
+                              void *dst, cudaStream_t stream) {
     const int nt = 256;
     const int64_t n = (int64_t)A * Fp;
-    pad_meas<<<(unsigned)((n + nt - 1) / nt), nt, 0, stream>>>(src, A, F, dst, Fp);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_interleave_pad(const float *re, const float *im, int A, int F, float2 *dst,
-                                  int Fp, cudaStream_t stream) {
-    const int nt = 256;
-    const int64_t n = (int64_t)A * Fp;
-    interleave_pad_meas<<<(unsigned)((n + nt - 1) / nt), nt, 0, stream>>>(re, im, A, F, dst, Fp);
+    stage_meas<<<(unsigned)((n + nt - 1) / nt), nt, 0, stream>>>(src, im, A, F, Fp, esz, dst);
     return cudaGetLastError();
 }
 

@@ -13,7 +13,7 @@ struct FwdParams {
     int64_t vox_start;     // first voxel of this launch
     int64_t vox_count;     // voxels in this launch (tiles cover [vox_start, +vox_count))
     const AntRec *ant;     // [num_ant]
-    const float2 *meas;    // [num_ant, fp] complex64, fp % 32 == 0, 16-byte aligned
+    const void *meas;      // [num_ant, fp] samples in the kernel form's layout (8 or 16 B each)
     int32_t num_ant;
     int32_t fp;
     int32_t ant_per_stage; // antennas per shared-memory stage
@@ -36,7 +36,9 @@ struct FwdVariant {
     int t;      // voxels per thread
     int nt;     // threads per CTA
     bool plain; // PLAIN form
+    int esz;    // bytes per staged sample: 8 (re, im) or 16 (re, re, im, im)
     const void *fn;
+    const char *name;
 };
 
 const FwdVariant *fwd_variants(int *count);
@@ -45,10 +47,8 @@ cudaError_t launch_fwd(const FwdVariant &var, const FwdParams &p, size_t smem,
 cudaError_t launch_reduce(const FwdParams &p, cudaStream_t stream);
 cudaError_t launch_prep_antennas(const float *ant, const float *rxo, int R, const float *pos_off,
                                  int A, AntRec *out, int32_t *mono_flag, cudaStream_t stream);
-cudaError_t launch_pad_meas(const float2 *src, int A, int F, float2 *dst, int Fp,
-                            cudaStream_t stream);
-cudaError_t launch_interleave_pad(const float *re, const float *im, int A, int F, float2 *dst,
-                                  int Fp, cudaStream_t stream);
+cudaError_t launch_stage_meas(const float *src, const float *im, int A, int F, int Fp, int esz,
+                              void *dst, cudaStream_t stream);
 
 // ---------------------------------------------------------- interpolated mode
 struct InterpParams {

@@ -25,7 +25,7 @@ constexpr int kMaxFp = 24576;  // one antenna row per stage still fits in shared
 
 inline size_t align_up(size_t x, size_t a = kAlign) { return (x + a - 1) / a * a; }
 
-std::atomic<int> g_variant[2] = {{0}, {4}};  // default variant per MIXED / PLAIN
+std::atomic<int> g_variant[2] = {{0}, {5}};  // default variant per MIXED / PLAIN
 
 struct FwdPlan {
     const FwdVariant *var;
@@ -60,11 +60,12 @@ int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int 
     const FwdVariant *vars = fwd_variants(&nvar);
     int vi = variant_index_for(mode);
     if (vi < 0 || vi >= nvar || vars[vi].plain != (mode == MMN_MODE_PLAIN))
-        vi = (mode == MMN_MODE_PLAIN) ? 4 : 0;
+        vi = (mode == MMN_MODE_PLAIN) ? 5 : 0;
     pl->var = &vars[vi];
     pl->fp = (F + kBlockF - 1) / kBlockF * kBlockF;
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
-    const int rec = (int)sizeof(AntRec) + pl->fp * (int)sizeof(float2);
+    const int esz = pl->var->esz;
+    const int rec = (int)sizeof(AntRec) + pl->fp * esz;
     pl->ant_per_stage = std::max(1, std::min(16, kMaxStageBytes / rec));
     pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec + (pl->var->plain ? pl->fp * 4 : 0);
     pl->vox_start = vox_start;
@@ -107,12 +108,12 @@ int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int 
         pl->ant_per_split = aps;
         pl->splits = (A + aps - 1) / aps;
     }
-    pl->copy_meas = !meas_aligned || pl->fp != F;
+    pl->copy_meas = esz != 8 || !meas_aligned || pl->fp != F;
     size_t off = kStatusBytes;
     pl->off_ant = off;
     off = align_up(off + (size_t)A * sizeof(AntRec));
     pl->off_meas = off;
-    if (pl->copy_meas) off = align_up(off + (size_t)A * pl->fp * sizeof(float2));
+    if (pl->copy_meas) off = align_up(off + (size_t)A * pl->fp * esz);
     pl->off_partial = off;
     if (pl->splits > 1 || want_partial_space)
         off = align_up(off + (size_t)pl->splits * (size_t)vox_count * 8 * sizeof(float));
@@ -132,14 +133,11 @@ int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
     e = launch_prep_antennas(p->antenna_locs, p->rx_offsets, p->num_rx, p->pos_offsets, A, ant,
                              hdr + 1, stream);
     if (e != cudaSuccess) return MMN_ERR_CUDA;
-    const float2 *meas = reinterpret_cast<const float2 *>(p->meas);
-    if (meas_r) {
-        float2 *dst = reinterpret_cast<float2 *>(ws + pl.off_meas);
-        e = launch_interleave_pad(meas_r, meas_i, A, F, dst, pl.fp, stream);
-        meas = dst;
-    } else if (pl.copy_meas) {
-        float2 *dst = reinterpret_cast<float2 *>(ws + pl.off_meas);
-        e = launch_pad_meas(meas, A, F, dst, pl.fp, stream);
+    const void *meas = p->meas;
+    if (meas_r || pl.copy_meas) {
+        void *dst = ws + pl.off_meas;
+        e = meas_r ? launch_stage_meas(meas_r, meas_i, A, F, pl.fp, pl.var->esz, dst, stream)
+                   : launch_stage_meas(p->meas, nullptr, A, F, pl.fp, pl.var->esz, dst, stream);
         meas = dst;
     }
     if (e != cudaSuccess) return MMN_ERR_CUDA;
@@ -237,6 +235,18 @@ int mmn_set_variant(int32_t mode, int32_t idx) {
         ++c;
     }
     return MMN_ERR_INVALID_ARGUMENT;
+}
+
+const char *mmn_variant_name(int32_t mode, int32_t idx) {
+    int n = 0;
+    const FwdVariant *v = fwd_variants(&n);
+    int c = 0;
+    for (int i = 0; i < n; ++i) {
+        if (v[i].plain != (mode == MMN_MODE_PLAIN)) continue;
+        if (c == idx) return v[i].name;
+        ++c;
+    }
+    return nullptr;
 }
 
 size_t mmn_workspace_bytes(const mmn_problem *p, int32_t mode, int32_t want_vote) {
@@ -356,7 +366,7 @@ size_t mmn_cuda_image_workspace_bytes(int num_antennas, int samples_per_meas,
     // 2^17-voxel launch plus the grid-independent part.  Callers that launch more
     // voxels should query with mmn_cuda_image_workspace_bytes_for.
     return align_up(kStatusBytes) + align_up((size_t)num_antennas * sizeof(AntRec)) +
-           align_up((size_t)num_antennas * fp * sizeof(float2));
+           align_up((size_t)num_antennas * fp * 16);
 }
 
 size_t mmn_cuda_image_workspace_bytes_for(int num_x, int num_y, int num_z, int num_antennas,
@@ -372,7 +382,7 @@ size_t mmn_cuda_image_workspace_bytes_for(int num_x, int num_y, int num_z, int n
     if (plan_forward(nvox, start_ind, count, num_antennas, samples_per_meas, MMN_MODE_MIXED,
                      false, false, &pl) != MMN_OK)
         return 0;
-    return pl.total;
+    return pl.total;  // SoA input: plan_forward with meas_aligned=false always stages
 }
 
 int mmn_cuda_image(float *p_xyz_r, float *p_xyz_i, const float *x_locs, const float *y_locs,

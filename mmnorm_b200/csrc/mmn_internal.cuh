@@ -58,6 +58,42 @@ __device__ __forceinline__ float2 cis_fp64_phase(double phi) {
     return make_float2(cr, sr);
 }
 
+// Two phases at once: the FP64 reduction per element as in cis_fp64_phase, the FP32
+// Taylor polynomials as packed FFMA2/FMUL2 on (element 0, element 1).  Returns
+// c = (cos phi0, cos phi1), s = (sin phi0, sin phi1), ns = -s.
+__device__ __forceinline__ void cis_fp64_phase_pair(double phi0, double phi1, float2 &c,
+                                                    float2 &s, float2 &ns) {
+    const double kTwoOverPi = 0.636619772367581343075535053490057448;
+    const double kPiOver2 = 1.570796326794896619231321691639751442;
+    const double kRound = 6755399441055744.0;  // 1.5 * 2^52
+    const double t0 = fma(phi0, kTwoOverPi, kRound);
+    const double t1 = fma(phi1, kTwoOverPi, kRound);
+    const int q0 = __double2loint(t0);
+    const int q1 = __double2loint(t1);
+    const double n0 = t0 - kRound, n1 = t1 - kRound;
+    const float2 x = make_float2((float)fma(-n0, kPiOver2, phi0), (float)fma(-n1, kPiOver2, phi1));
+    const float2 x2 = __fmul2_rn(x, x);
+    const float2 x3 = __fmul2_rn(x2, x);
+    float2 sp = __ffma2_rn(x2, make_float2(2.75573192239858906526e-6f, 2.75573192239858906526e-6f),
+                           make_float2(-1.98412698412698412698e-4f, -1.98412698412698412698e-4f));
+    sp = __ffma2_rn(x2, sp, make_float2(8.33333333333333333333e-3f, 8.33333333333333333333e-3f));
+    sp = __ffma2_rn(x2, sp, make_float2(-1.66666666666666666667e-1f, -1.66666666666666666667e-1f));
+    sp = __ffma2_rn(x3, sp, x);
+    float2 cp = __ffma2_rn(x2, make_float2(-2.75573192239858906526e-7f, -2.75573192239858906526e-7f),
+                           make_float2(2.48015873015873015873e-5f, 2.48015873015873015873e-5f));
+    cp = __ffma2_rn(x2, cp, make_float2(-1.38888888888888888889e-3f, -1.38888888888888888889e-3f));
+    cp = __ffma2_rn(x2, cp, make_float2(4.16666666666666666667e-2f, 4.16666666666666666667e-2f));
+    cp = __ffma2_rn(x2, cp, make_float2(-0.5f, -0.5f));
+    cp = __ffma2_rn(x2, cp, make_float2(1.0f, 1.0f));
+    float s0 = (q0 & 1) ? cp.x : sp.x, c0 = (q0 & 1) ? -sp.x : cp.x;
+    float s1 = (q1 & 1) ? cp.y : sp.y, c1 = (q1 & 1) ? -sp.y : cp.y;
+    if (q0 & 2) { s0 = -s0; c0 = -c0; }
+    if (q1 & 2) { s1 = -s1; c1 = -c1; }
+    c = make_float2(c0, c1);
+    s = make_float2(s0, s1);
+    ns = make_float2(-s0, -s1);
+}
+
 // FP64 round-trip distance TX -> v -> RX.  `mono` (all RX offsets zero) reuses the
 // forward leg for the return leg, which is bit-identical to computing it again.
 __device__ __forceinline__ double range_fp64(double vx, double vy, double vz,

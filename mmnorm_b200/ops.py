@@ -162,7 +162,9 @@ def variants(mode="mixed"):
         t, nt = ctypes.c_int32(), ctypes.c_int32()
         _lib.check(lib.mmn_variant_info(m, i, ctypes.byref(t), ctypes.byref(nt)),
                    "mmn_variant_info")
-        out.append({"index": i, "voxels_per_thread": t.value, "threads": nt.value})
+        name = lib.mmn_variant_name(m, i)
+        out.append({"index": i, "name": name.decode() if name else None,
+                    "voxels_per_thread": t.value, "threads": nt.value})
     return out
 
 

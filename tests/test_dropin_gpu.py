@@ -59,10 +59,9 @@ def test_interp_mode_image_and_normals(cuda_dev, oracle, R, use_4_rx, ti):
                                        use_interpolated_processing=True, dist_mode=1)
     assert oracle.rel_l2(img, ref) < 5e-4
     np.testing.assert_array_equal(centres, ref_c)
-    nrm = py_sn_est_gpu.normal_estimates_cuda(img, *args[1:], use_4_rx=use_4_rx,
-                                              is_ti_radar=ti)
-    nref = oracle.ref_normal_estimates_cuda(img, *args[1:], use_4_rx=use_4_rx,
-                                            is_ti_radar=ti, dist_mode=1)
+    nrm = py_sn_est_gpu.normal_estimates_cuda(img, *args, use_4_rx=use_4_rx, is_ti_radar=ti)
+    nref = oracle.ref_normal_estimates_cuda(img, *args, use_4_rx=use_4_rx, is_ti_radar=ti,
+                                            dist_mode=1)
     assert nrm.dtype == np.float64 and nrm.shape == sc.grid_shape + (3,)
     np.testing.assert_array_equal(np.isnan(nrm), np.isnan(nref))
     ok = ~np.isnan(nref[..., 0])
@@ -101,7 +100,7 @@ def test_full_mode_normals_and_pipeline(cuda_dev, oracle):
     args = (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs.astype(np.float64), data, rxo,
             sc.slope, sc.wavelength, sc.f_hi - sc.f_lo, sc.num_freqs)
     img, _ = py_image_gpu.image_cuda(*args, use_4_rx=True)
-    raw = py_sn_est_gpu.normal_estimates_cuda(img, *args[1:], use_4_rx=True,
+    raw = py_sn_est_gpu.normal_estimates_cuda(img, *args, use_4_rx=True,
                                               use_interpolated_processing=False)
     Io, Wo = oracle.full(sc.voxel_centres(), sc.antenna_locs, rxo, sc.meas, sc.wavelength,
                          sc.slope)

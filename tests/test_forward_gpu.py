@@ -147,12 +147,12 @@ def test_deterministic_and_status_clean(cuda_dev):
     assert ops.read_status(ws) == 0
 
 
-@pytest.mark.parametrize("idx", [0, 1, 2, 3])
+@pytest.mark.parametrize("idx", [0, 1, 2, 3, 4, 5])
 def test_every_mixed_variant(cuda_dev, oracle, idx):
     from mmnorm_b200 import ops
     n = len(ops.variants("mixed"))
     if idx >= n:
-        pytest.skip("variant not built")
+        pytest.skip("no variant %d" % idx)
     ops.set_variant("mixed", idx)
     try:
         sc = small_scene(seed=10, n_vox=9)
@@ -198,3 +198,53 @@ def test_config0_subset_and_normals(cuda_dev, oracle):
     ang = oracle.angle_deg(n[sel], raw_o[pos])
     assert np.median(ang) < 0.5
     assert np.all(np.isnan(n[~mask]))
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_every_plain_variant(cuda_dev, oracle, idx):
+    from mmnorm_b200 import ops
+    if idx >= len(ops.variants("plain")):
+        pytest.skip("no variant %d" % idx)
+    ops.set_variant("plain", idx)
+    try:
+        sc = small_scene(seed=15, n_vox=7)
+        I, W = run_ops(cuda_dev, sc, "plain")
+    finally:
+        ops.set_variant("plain", 0)
+    Io, Wo = oracle.full(sc.voxel_centres(), sc.antenna_locs, np.zeros((1, 3)), sc.meas,
+                         sc.wavelength, sc.slope)
+    assert oracle.rel_l2(I, Io) < TOL_PLAIN
+    assert oracle.rel_l2(W, Wo) < TOL_PLAIN
+
+
+def test_pair_and_scalar_mixed_forms_agree_bitwise(cuda_dev):
+    """FFMA2 computes each half with a single rounding, exactly like FFMA: the paired
+    and the scalar mixed kernels produce identical bits."""
+    from mmnorm_b200 import ops
+    names = [v["name"] for v in ops.variants("mixed")]
+    i_pair = names.index("mixed_ffma2_t4_n128")
+    i_scal = names.index("mixed_ffma_t4_n128")
+    sc = scenes.sphere_scene(seed=16, n_ap=12, nf=64, n_vox=11, n_pts=20)
+    out = []
+    for idx in (i_pair, i_scal):
+        ops.set_variant("mixed", idx)
+        try:
+            out.append(run_ops(cuda_dev, sc, "mixed"))
+        finally:
+            ops.set_variant("mixed", 0)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_autotuner_selects_a_variant(cuda_dev):
+    import torch
+    from mmnorm_b200 import autotune, ops
+    sc = scenes.sphere_scene(seed=17, n_ap=16, nf=64, n_vox=16, n_pts=20)
+    args = [_t(v, cuda_dev) for v in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs,
+                                      np.zeros((1, 3), np.float32), sc.meas)]
+    res = autotune.tune(*args, sc.wavelength, sc.slope, mode="mixed", max_antennas=64)
+    try:
+        assert res["best"] in range(len(ops.variants("mixed")))
+        assert len(res["times_ms"]) == len(ops.variants("mixed"))
+    finally:
+        ops.set_variant("mixed", 0)

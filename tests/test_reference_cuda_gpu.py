@@ -161,7 +161,7 @@ def test_full_mode_vs_reference_kernel(cuda_dev, ref_cuda, oracle):
     ours = _mmn_cuda_image(d, False, cuda_dev)
     ref_c = ref[0] + 1j * ref[1]
     ours_c = ours[0] + 1j * ours[1]
-    Io, _ = oracle.full(sc.voxel_centres(), sc.antenna_locs, np.zeros((1, 3)), m,
+    Io, _ = oracle.full(sc.voxel_centres(), sc.antenna_locs, d["rxo_np"], m,
                         float(d["wl"]), float(d["slope"]), vote=False)
     e_ours = oracle.rel_l2(ours_c, Io)
     e_ref = oracle.rel_l2(ref_c, Io)
