@@ -46,6 +46,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU seconds of the bounded reference/CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--variant", default=None,
+                    help="force a mixed kernel variant by name instead of autotuning")
     ap.add_argument("--aperture", type=int, default=128,
                     help="aperture side (antennas); smaller values make a profiling case "
                          "with the same kernel and voxel grid (the default is the workload)")
@@ -239,7 +241,12 @@ def ours_arm(args):
     xs, ys, zs = t(sc.x_locs), t(sc.y_locs), t(sc.z_locs)
     ant, rxo = t(sc.antenna_locs), t(np.zeros((1, 3), np.float32))
     meas = t(sc.meas)
-    tuned = autotune.tune(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope, mode="mixed")
+    if args.variant:
+        names = [v["name"] for v in ops.variants("mixed")]
+        ops.set_variant("mixed", names.index(args.variant))
+        tuned = {"best": names.index(args.variant), "times_ms": None}
+    else:
+        tuned = autotune.tune(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope, mode="mixed")
     variant = ops.variants("mixed")[tuned["best"]]
     prob = ops.make_problem(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope)
     ws = torch.empty(ops.workspace_bytes(prob, "mixed"), dtype=torch.uint8, device=dev)

@@ -110,6 +110,7 @@ __device__ __forceinline__ void store_voxel(const FwdParams &p, int split, int64
 constexpr int kFormMixedPair = 0;    // FFMA2 voxel pairs, (re,re,im,im) samples
 constexpr int kFormMixedScalar = 1;  // scalar FFMA, (re,im) samples
 constexpr int kFormPlain = 2;        // FP32 sincosf per sample, (re,im) samples
+constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im_a') samples
 
 template <int T, int NT, int FORM>
 __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
     st.bars = reinterpret_cast<uint64_t *>(smem);
     st.base = smem + 128;
     st.nas = p.ant_per_stage;
-    st.esz = FORM == kFormMixedPair ? 16 : 8;
+    st.esz = FORM == kFormMixedPair ? 16 : 8;  // antenna pairs: 16 B per pair = 8 B per antenna
     st.fp = p.fp;
     st.stage_bytes = (size_t)st.nas * sizeof(AntRec) + (size_t)st.nas * st.fp * st.esz;
     float *kappa_tab = reinterpret_cast<float *>(st.base + 2 * st.stage_bytes);  // PLAIN only
@@ -167,6 +168,75 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
         const unsigned char *mstage = st.meas(s);
         const int na = min(st.nas, a_end - (a_begin + c * st.nas));
 
+        if constexpr (FORM == kFormMixedAntPair) {
+            // antennas (2pp, 2pp+1) ride in the two halves of every FFMA2
+            const float4 *m4base = reinterpret_cast<const float4 *>(mstage);
+            for (int pp = 0; pp < na / 2; ++pp) {
+                const AntRec &a0r = ants[2 * pp];
+                const AntRec &a1r = ants[2 * pp + 1];
+                const float4 *m4 = m4base + (size_t)pp * fp;
+                double d0[T], d1[T];
+                float2 zr[T], zi[T], nzi[T], c2r[T], c2i[T];
+#pragma unroll
+                for (int k = 0; k < T; ++k) {
+                    const double x = vx[k], y = vy[k], z = vz[k];
+                    d0[k] = range_fp64(x, y, z, a0r, mono, p.ti);
+                    d1[k] = range_fp64(x, y, z, a1r, mono, p.ti);
+                    cis_fp64_phase_pair(-d0[k] * p.kd, -d1[k] * p.kd, zr[k], zi[k], nzi[k]);
+                    c2r[k] = c2i[k] = make_float2(0.f, 0.f);
+                }
+                for (int b = 0; b < nblk; ++b) {
+                    const float4 *mb = m4 + b * kBlockF;
+                    float2 hr[T], hi[T];
+                    const float4 top = mb[kBlockF - 1];
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        hr[k] = make_float2(top.x, top.y);
+                        hi[k] = make_float2(top.z, top.w);
+                    }
+#pragma unroll
+                    for (int t = kBlockF - 2; t >= 0; --t) {
+                        const float4 mm = mb[t];
+                        const float2 mr = make_float2(mm.x, mm.y), mi = make_float2(mm.z, mm.w);
+#pragma unroll
+                        for (int k = 0; k < T; ++k) {
+                            const float2 u = __ffma2_rn(hr[k], zr[k], mr);
+                            const float2 w = __ffma2_rn(hr[k], zi[k], mi);
+                            hr[k] = __ffma2_rn(hi[k], nzi[k], u);
+                            hi[k] = __ffma2_rn(hi[k], zr[k], w);
+                        }
+                    }
+                    const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        float2 anr, ani, nani;
+                        cis_fp64_phase_pair(-d0[k] * kap, -d1[k] * kap, anr, ani, nani);
+                        c2r[k] = __ffma2_rn(anr, hr[k], __ffma2_rn(nani, hi[k], c2r[k]));
+                        c2i[k] = __ffma2_rn(anr, hi[k], __ffma2_rn(ani, hr[k], c2i[k]));
+                    }
+                }
+                // image + vote, antenna 2pp then 2pp+1 (the scalar kernels' order)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const AntRec &ar = h ? a1r : a0r;
+                    const float ux0 = ar.virt[0], uy0 = ar.virt[1], uz0 = ar.virt[2];
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        const float cr = h ? c2r[k].y : c2r[k].x;
+                        const float ci = h ? c2i[k].y : c2i[k].x;
+                        const float ux = ux0 - vx[k], uy = uy0 - vy[k], uz = uz0 - vz[k];
+                        acc[k][0] += cr;
+                        acc[k][1] += ci;
+                        acc[k][2] = fmaf(cr, ux, acc[k][2]);
+                        acc[k][3] = fmaf(ci, ux, acc[k][3]);
+                        acc[k][4] = fmaf(cr, uy, acc[k][4]);
+                        acc[k][5] = fmaf(ci, uy, acc[k][5]);
+                        acc[k][6] = fmaf(cr, uz, acc[k][6]);
+                        acc[k][7] = fmaf(ci, uz, acc[k][7]);
+                    }
+                }
+            }
+        } else
         for (int a = 0; a < na; ++a) {
             const AntRec &ar = ants[a];
             float cr[T], ci[T];
@@ -354,7 +424,7 @@ __global__ void bp_reduce_partials(const FwdParams p) {
 // does (surface_normal_est.cu:128-130).  Thread 0 also records whether every RX offset
 // is zero (the forward kernels then reuse the outgoing leg for the return leg).
 __global__ void prep_antennas(const float *__restrict__ ant, const float *__restrict__ rxo,
-                              int R, const float *__restrict__ pos_off, int A,
+                              int R, const float *__restrict__ pos_off, int A, int A_pad,
                               AntRec *__restrict__ out, int32_t *__restrict__ mono_flag) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -362,16 +432,19 @@ __global__ void prep_antennas(const float *__restrict__ ant, const float *__rest
         for (int q = 0; q < 3 * R; ++q) mono &= (rxo[q] == 0.f);
         *mono_flag = mono;
     }
-    if (i >= A) return;
+    if (i >= A_pad) return;
+    // records past A (padding to an even count) repeat the last antenna; their staged
+    // samples are zero, so they contribute exactly nothing
+    const int src = i < A ? i : A - 1;
     AntRec r;
-    const int q = i % R;
+    const int q = src % R;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        float a = ant[3 * i + k];
+        float a = ant[3 * src + k];
         double ad = a;
         if (pos_off) {
-            ad += (double)pos_off[3 * i + k];
-            a = a + pos_off[3 * i + k];
+            ad += (double)pos_off[3 * src + k];
+            a = a + pos_off[3 * src + k];
         }
         const float o = rxo[3 * q + k];
         r.tx[k] = ad;
@@ -385,28 +458,34 @@ __global__ void prep_antennas(const float *__restrict__ ant, const float *__rest
 // Measurement rows [A, F] (complex64, or SoA planes re/im when `im` is non-null) into
 // the shared-memory layout of a kernel form: rows of Fp = roundup(F, 32) samples,
 // zero-padded (zero samples at the top of a Horner block add exactly nothing), each
-// sample either (re, im) (esz 8) or (re, re, im, im) (esz 16).
+// sample either
+//   layout 0: (re, im)                       8 B per antenna-sample
+//   layout 1: (re, re, im, im)              16 B per antenna-sample (voxel pairs)
+//   layout 2: (re_a, re_a', im_a, im_a')    16 B per antenna PAIR-sample (antenna pairs
+//             a = 2p, a' = 2p+1; an antenna index >= A is zero)
+__device__ __forceinline__ float2 load_sample(const float *src, const float *im, int A, int F,
+                                              int64_t a, int j) {
+    if (a >= A || j >= F) return make_float2(0.f, 0.f);
+    if (im) return make_float2(src[a * F + j], im[a * F + j]);
+    return reinterpret_cast<const float2 *>(src)[a * F + j];
+}
+
 __global__ void stage_meas(const float *__restrict__ src, const float *__restrict__ im, int A,
-                           int F, int Fp, int esz, void *__restrict__ dst) {
+                           int F, int Fp, int layout, int rows, void *__restrict__ dst) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)A * Fp) return;
-    const int64_t a = idx / Fp;
-    const int j = (int)(idx - a * Fp);
-    float re = 0.f, ig = 0.f;
-    if (j < F) {
-        if (im) {
-            re = src[a * F + j];
-            ig = im[a * F + j];
-        } else {
-            const float2 m = reinterpret_cast<const float2 *>(src)[a * F + j];
-            re = m.x;
-            ig = m.y;
-        }
+    if (idx >= (int64_t)rows * Fp) return;
+    const int64_t r = idx / Fp;
+    const int j = (int)(idx - r * Fp);
+    if (layout == 2) {
+        const float2 m0 = load_sample(src, im, A, F, 2 * r, j);
+        const float2 m1 = load_sample(src, im, A, F, 2 * r + 1, j);
+        reinterpret_cast<float4 *>(dst)[idx] = make_float4(m0.x, m1.x, m0.y, m1.y);
+    } else if (layout == 1) {
+        const float2 m = load_sample(src, im, A, F, r, j);
+        reinterpret_cast<float4 *>(dst)[idx] = make_float4(m.x, m.x, m.y, m.y);
+    } else {
+        reinterpret_cast<float2 *>(dst)[idx] = load_sample(src, im, A, F, r, j);
     }
-    if (esz == 16)
-        reinterpret_cast<float4 *>(dst)[idx] = make_float4(re, re, ig, ig);
-    else
-        reinterpret_cast<float2 *>(dst)[idx] = make_float2(re, ig);
 }
 
 // ------------------------------------------------------------------ instantiations
@@ -418,14 +497,16 @@ static const void *fwd_ptr() {
 const FwdVariant *fwd_variants(int *count) {
     // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
-        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair>(), "mixed_ffma2_t4_n128"},
-        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPair>(), "mixed_ffma2_t2_n128"},
-        {4, 256, false, 16, fwd_ptr<4, 256, kFormMixedPair>(), "mixed_ffma2_t4_n256"},
-        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair>(), "mixed_ffma2_t2_n256"},
-        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedScalar>(), "mixed_ffma_t4_n128"},
-        {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128"},
-        {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128"},
-        {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256"},
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair>(), "mixed_antpair_t2_n256", 2},
+        {2, 128, false, 8, fwd_ptr<2, 128, kFormMixedAntPair>(), "mixed_antpair_t2_n128", 2},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedAntPair>(), "mixed_antpair_t4_n128", 2},
+        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair>(), "mixed_antpair_t1_n256", 2},
+        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair>(), "mixed_ffma2_t4_n128", 1},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair>(), "mixed_ffma2_t2_n256", 1},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedScalar>(), "mixed_ffma_t4_n128", 0},
+        {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256", 0},
+        {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128", 0},
+        {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128", 0},
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
     return v;
@@ -446,17 +527,21 @@ cudaError_t launch_reduce(const FwdParams &p, cudaStream_t stream) {
 }
 
 cudaError_t launch_prep_antennas(const float *ant, const float *rxo, int R, const float *pos_off,
-                                 int A, AntRec *out, int32_t *mono_flag, cudaStream_t stream) {
+                                 int A, int A_pad, AntRec *out, int32_t *mono_flag,
+                                 cudaStream_t stream) {
     const int nt = 256;
-    prep_antennas<<<(A + nt) / nt, nt, 0, stream>>>(ant, rxo, R, pos_off, A, out, mono_flag);
+    prep_antennas<<<(A_pad + nt) / nt, nt, 0, stream>>>(ant, rxo, R, pos_off, A, A_pad, out,
+                                                         mono_flag);
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage_meas(const float *src, const float *im, int A, int F, int Fp, int esz,
-                              void *dst, cudaStream_t stream) {
+cudaError_t launch_stage_meas(const float *src, const float *im, int A, int F, int Fp,
+                              int layout, void *dst, cudaStream_t stream) {
     const int nt = 256;
-    const int64_t n = (int64_t)A * Fp;
-    stage_meas<<<(unsigned)((n + nt - 1) / nt), nt, 0, stream>>>(src, im, A, F, Fp, esz, dst);
+    const int rows = layout == 2 ? (A + 1) / 2 : A;
+    const int64_t n = (int64_t)rows * Fp;
+    stage_meas<<<(unsigned)((n + nt - 1) / nt), nt, 0, stream>>>(src, im, A, F, Fp, layout, rows,
+                                                                 dst);
     return cudaGetLastError();
 }
 

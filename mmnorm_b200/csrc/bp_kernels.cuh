@@ -36,9 +36,10 @@ struct FwdVariant {
     int t;      // voxels per thread
     int nt;     // threads per CTA
     bool plain; // PLAIN form
-    int esz;    // bytes per staged sample: 8 (re, im) or 16 (re, re, im, im)
+    int esz;    // staged bytes per antenna-sample: 8 or 16
     const void *fn;
     const char *name;
+    int layout; // staged sample layout (stage_meas): 0 (re,im), 1 (re,re,im,im), 2 antenna pairs
 };
 
 const FwdVariant *fwd_variants(int *count);
@@ -46,9 +47,10 @@ cudaError_t launch_fwd(const FwdVariant &var, const FwdParams &p, size_t smem,
                        cudaStream_t stream);
 cudaError_t launch_reduce(const FwdParams &p, cudaStream_t stream);
 cudaError_t launch_prep_antennas(const float *ant, const float *rxo, int R, const float *pos_off,
-                                 int A, AntRec *out, int32_t *mono_flag, cudaStream_t stream);
-cudaError_t launch_stage_meas(const float *src, const float *im, int A, int F, int Fp, int esz,
-                              void *dst, cudaStream_t stream);
+                                 int A, int A_pad, AntRec *out, int32_t *mono_flag,
+                                 cudaStream_t stream);
+cudaError_t launch_stage_meas(const float *src, const float *im, int A, int F, int Fp,
+                              int layout, void *dst, cudaStream_t stream);
 
 // ---------------------------------------------------------- interpolated mode
 struct InterpParams {

@@ -25,11 +25,11 @@ constexpr int kMaxFp = 24576;  // one antenna row per stage still fits in shared
 
 inline size_t align_up(size_t x, size_t a = kAlign) { return (x + a - 1) / a * a; }
 
-std::atomic<int> g_variant[2] = {{0}, {5}};  // default variant per MIXED / PLAIN
+std::atomic<int> g_variant[2] = {{-1}, {-1}};  // selected variant per MIXED / PLAIN; -1: first
 
 struct FwdPlan {
     const FwdVariant *var;
-    int fp, ant_per_stage, tiles, splits, ant_per_split;
+    int fp, ant_per_stage, tiles, splits, ant_per_split, a_pad;
     size_t smem;
     int64_t vox_start, vox_count;
     bool copy_meas;
@@ -59,14 +59,20 @@ int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int 
     int nvar = 0;
     const FwdVariant *vars = fwd_variants(&nvar);
     int vi = variant_index_for(mode);
-    if (vi < 0 || vi >= nvar || vars[vi].plain != (mode == MMN_MODE_PLAIN))
-        vi = (mode == MMN_MODE_PLAIN) ? 5 : 0;
+    if (vi < 0 || vi >= nvar || vars[vi].plain != (mode == MMN_MODE_PLAIN)) {
+        vi = 0;
+        while (vi < nvar && vars[vi].plain != (mode == MMN_MODE_PLAIN)) ++vi;
+    }
     pl->var = &vars[vi];
+    const bool pairs = pl->var->layout == 2;
+    pl->a_pad = pairs ? A + (A & 1) : A;
+    A = pl->a_pad;
     pl->fp = (F + kBlockF - 1) / kBlockF * kBlockF;
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
     const int esz = pl->var->esz;
     const int rec = (int)sizeof(AntRec) + pl->fp * esz;
     pl->ant_per_stage = std::max(1, std::min(16, kMaxStageBytes / rec));
+    if (pairs) pl->ant_per_stage = std::max(2, pl->ant_per_stage & ~1);
     pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec + (pl->var->plain ? pl->fp * 4 : 0);
     pl->vox_start = vox_start;
     pl->vox_count = vox_count;
@@ -108,10 +114,10 @@ int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int 
         pl->ant_per_split = aps;
         pl->splits = (A + aps - 1) / aps;
     }
-    pl->copy_meas = esz != 8 || !meas_aligned || pl->fp != F;
+    pl->copy_meas = pl->var->layout != 0 || !meas_aligned || pl->fp != F;
     size_t off = kStatusBytes;
     pl->off_ant = off;
-    off = align_up(off + (size_t)A * sizeof(AntRec));
+    off = align_up(off + (size_t)A * sizeof(AntRec));  // A is the padded count here
     pl->off_meas = off;
     if (pl->copy_meas) off = align_up(off + (size_t)A * pl->fp * esz);
     pl->off_partial = off;
@@ -130,14 +136,14 @@ int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
     if (e != cudaSuccess) return MMN_ERR_CUDA;
     AntRec *ant = reinterpret_cast<AntRec *>(ws + pl.off_ant);
     int32_t *hdr = reinterpret_cast<int32_t *>(ws);
-    e = launch_prep_antennas(p->antenna_locs, p->rx_offsets, p->num_rx, p->pos_offsets, A, ant,
-                             hdr + 1, stream);
+    e = launch_prep_antennas(p->antenna_locs, p->rx_offsets, p->num_rx, p->pos_offsets, A,
+                             pl.a_pad, ant, hdr + 1, stream);
     if (e != cudaSuccess) return MMN_ERR_CUDA;
     const void *meas = p->meas;
     if (meas_r || pl.copy_meas) {
         void *dst = ws + pl.off_meas;
-        e = meas_r ? launch_stage_meas(meas_r, meas_i, A, F, pl.fp, pl.var->esz, dst, stream)
-                   : launch_stage_meas(p->meas, nullptr, A, F, pl.fp, pl.var->esz, dst, stream);
+        e = meas_r ? launch_stage_meas(meas_r, meas_i, A, F, pl.fp, pl.var->layout, dst, stream)
+                   : launch_stage_meas(p->meas, nullptr, A, F, pl.fp, pl.var->layout, dst, stream);
         meas = dst;
     }
     if (e != cudaSuccess) return MMN_ERR_CUDA;
@@ -155,7 +161,7 @@ int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
     fp.vox_count = pl.vox_count;
     fp.ant = ant;
     fp.meas = meas;
-    fp.num_ant = A;
+    fp.num_ant = pl.a_pad;
     fp.fp = pl.fp;
     fp.ant_per_stage = pl.ant_per_stage;
     fp.mono_flag = hdr + 1;

@@ -147,7 +147,7 @@ def test_deterministic_and_status_clean(cuda_dev):
     assert ops.read_status(ws) == 0
 
 
-@pytest.mark.parametrize("idx", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("idx", list(range(8)))
 def test_every_mixed_variant(cuda_dev, oracle, idx):
     from mmnorm_b200 import ops
     n = len(ops.variants("mixed"))
@@ -217,23 +217,27 @@ def test_every_plain_variant(cuda_dev, oracle, idx):
     assert oracle.rel_l2(W, Wo) < TOL_PLAIN
 
 
-def test_pair_and_scalar_mixed_forms_agree_bitwise(cuda_dev):
-    """FFMA2 computes each half with a single rounding, exactly like FFMA: the paired
-    and the scalar mixed kernels produce identical bits."""
+@pytest.mark.parametrize("n_ap", [12, 7])
+def test_pair_and_scalar_mixed_forms_agree_bitwise(cuda_dev, n_ap):
+    """FFMA2 computes each half with a single rounding, exactly like FFMA, and every form
+    accumulates a voxel's antennas in antenna order: the voxel-pair, antenna-pair and
+    scalar mixed kernels produce identical bits (n_ap=7: an odd antenna count, padded
+    with a zero antenna by the antenna-pair form)."""
     from mmnorm_b200 import ops
     names = [v["name"] for v in ops.variants("mixed")]
-    i_pair = names.index("mixed_ffma2_t4_n128")
-    i_scal = names.index("mixed_ffma_t4_n128")
-    sc = scenes.sphere_scene(seed=16, n_ap=12, nf=64, n_vox=11, n_pts=20)
+    picks = [names.index(n) for n in ("mixed_ffma_t4_n128", "mixed_ffma2_t4_n128",
+                                      "mixed_antpair_t2_n256", "mixed_antpair_t1_n256")]
+    sc = scenes.sphere_scene(seed=16, n_ap=n_ap, nf=64, n_vox=11, n_pts=20)
     out = []
-    for idx in (i_pair, i_scal):
+    for idx in picks:
         ops.set_variant("mixed", idx)
         try:
             out.append(run_ops(cuda_dev, sc, "mixed"))
         finally:
             ops.set_variant("mixed", 0)
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1])
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0])
+        assert np.array_equal(out[0][1], o[1])
 
 
 def test_autotuner_selects_a_variant(cuda_dev):
