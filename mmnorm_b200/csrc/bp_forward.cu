@@ -112,7 +112,14 @@ constexpr int kFormMixedScalar = 1;  // scalar FFMA, (re,im) samples
 constexpr int kFormPlain = 2;        // FP32 sincosf per sample, (re,im) samples
 constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im_a') samples
 
-template <int T, int NT, int FORM>
+// Block anchors: kAnchorPoly recomputes exp(-j d kappa_{32b}) per block from the FP64
+// phase (FP64 quarter-turn reduction + FP32 Taylor polynomials); kAnchorFixed steps a
+// 64-bit fixed-point phase accumulator per block and evaluates the hardware sine/cosine
+// on the wrapped angle.
+constexpr int kAnchorPoly = 0;
+constexpr int kAnchorFixed = 1;
+
+template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
 __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
     static_assert(FORM != kFormMixedPair || T % 2 == 0, "pair form needs an even T");
     extern __shared__ __align__(128) unsigned char smem[];
@@ -176,6 +183,7 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                 const AntRec &a1r = ants[2 * pp + 1];
                 const float4 *m4 = m4base + (size_t)pp * fp;
                 double d0[T], d1[T];
+                unsigned long long ph0[T], ph1[T], st0[T], st1[T];
                 float2 zr[T], zi[T], nzi[T], c2r[T], c2i[T];
 #pragma unroll
                 for (int k = 0; k < T; ++k) {
@@ -184,6 +192,12 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                     d1[k] = range_fp64(x, y, z, a1r, mono, p.ti);
                     cis_fp64_phase_pair(-d0[k] * p.kd, -d1[k] * p.kd, zr[k], zi[k], nzi[k]);
                     c2r[k] = c2i[k] = make_float2(0.f, 0.f);
+                    if constexpr (ANCHOR == kAnchorFixed) {
+                        ph0[k] = turns_to_fixed(-d0[k] * p.t0);
+                        ph1[k] = turns_to_fixed(-d1[k] * p.t0);
+                        st0[k] = turns_to_fixed(-d0[k] * p.tblk);
+                        st1[k] = turns_to_fixed(-d1[k] * p.tblk);
+                    }
                 }
                 for (int b = 0; b < nblk; ++b) {
                     const float4 *mb = m4 + b * kBlockF;
@@ -206,11 +220,19 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                             hi[k] = __ffma2_rn(hi[k], zr[k], w);
                         }
                     }
-                    const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
                         float2 anr, ani, nani;
-                        cis_fp64_phase_pair(-d0[k] * kap, -d1[k] * kap, anr, ani, nani);
+                        if constexpr (ANCHOR == kAnchorFixed) {
+                            fixed_cis(ph0[k], anr.x, ani.x);
+                            fixed_cis(ph1[k], anr.y, ani.y);
+                            nani = make_float2(-ani.x, -ani.y);
+                            ph0[k] += st0[k];
+                            ph1[k] += st1[k];
+                        } else {
+                            const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
+                            cis_fp64_phase_pair(-d0[k] * kap, -d1[k] * kap, anr, ani, nani);
+                        }
                         c2r[k] = __ffma2_rn(anr, hr[k], __ffma2_rn(nani, hi[k], c2r[k]));
                         c2i[k] = __ffma2_rn(anr, hi[k], __ffma2_rn(ani, hr[k], c2i[k]));
                     }
@@ -244,10 +266,16 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                 constexpr int P = T / 2;
                 const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * fp;
                 double d[T];
+                unsigned long long ph[T], stp[T];
                 float2 zr[P], zi[P], nzi[P], c2r[P], c2i[P];
 #pragma unroll
-                for (int k = 0; k < T; ++k)
+                for (int k = 0; k < T; ++k) {
                     d[k] = range_fp64((double)vx[k], (double)vy[k], (double)vz[k], ar, mono, p.ti);
+                    if constexpr (ANCHOR == kAnchorFixed) {
+                        ph[k] = turns_to_fixed(-d[k] * p.t0);
+                        stp[k] = turns_to_fixed(-d[k] * p.tblk);
+                    }
+                }
 #pragma unroll
                 for (int q = 0; q < P; ++q) {
                     cis_fp64_phase_pair(-d[2 * q] * p.kd, -d[2 * q + 1] * p.kd, zr[q], zi[q], nzi[q]);
@@ -274,11 +302,20 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
                             hi[q] = __ffma2_rn(hi[q], zr[q], w);
                         }
                     }
-                    const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
 #pragma unroll
                     for (int q = 0; q < P; ++q) {
                         float2 anr, ani, nani;
-                        cis_fp64_phase_pair(-d[2 * q] * kap, -d[2 * q + 1] * kap, anr, ani, nani);
+                        if constexpr (ANCHOR == kAnchorFixed) {
+                            fixed_cis(ph[2 * q], anr.x, ani.x);
+                            fixed_cis(ph[2 * q + 1], anr.y, ani.y);
+                            nani = make_float2(-ani.x, -ani.y);
+                            ph[2 * q] += stp[2 * q];
+                            ph[2 * q + 1] += stp[2 * q + 1];
+                        } else {
+                            const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
+                            cis_fp64_phase_pair(-d[2 * q] * kap, -d[2 * q + 1] * kap, anr, ani,
+                                                nani);
+                        }
                         c2r[q] = __ffma2_rn(anr, hr[q], __ffma2_rn(nani, hi[q], c2r[q]));
                         c2i[q] = __ffma2_rn(anr, hi[q], __ffma2_rn(ani, hr[q], c2i[q]));
                     }
@@ -489,14 +526,18 @@ __global__ void stage_meas(const float *__restrict__ src, const float *__restric
 }
 
 // ------------------------------------------------------------------ instantiations
-template <int T, int NT, int FORM>
+template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
 static const void *fwd_ptr() {
-    return reinterpret_cast<const void *>(&bp_fwd_kernel<T, NT, FORM>);
+    return reinterpret_cast<const void *>(&bp_fwd_kernel<T, NT, FORM, ANCHOR>);
 }
 
 const FwdVariant *fwd_variants(int *count) {
     // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256", 1},
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t2_n256", 2},
+        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t1_n256", 2},
+        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t4_n128", 1},
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair>(), "mixed_antpair_t2_n256", 2},
         {2, 128, false, 8, fwd_ptr<2, 128, kFormMixedAntPair>(), "mixed_antpair_t2_n128", 2},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedAntPair>(), "mixed_antpair_t4_n128", 2},

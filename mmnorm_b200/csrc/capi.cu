@@ -167,6 +167,8 @@ int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
     fp.mono_flag = hdr + 1;
     fp.k0 = 2.0 * kPi / p->wavelength;
     fp.kd = 2.0 * kPi * p->slope / kC;
+    fp.t0 = 1.0 / p->wavelength;
+    fp.tblk = (double)kBlockF * p->slope / kC;
     fp.ti = p->is_ti_radar ? 0.15 : 0.0;
     fp.num_tiles = pl.tiles;
     fp.num_splits = pl.splits;

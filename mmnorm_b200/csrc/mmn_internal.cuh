@@ -94,6 +94,25 @@ __device__ __forceinline__ void cis_fp64_phase_pair(double phi0, double phi1, fl
     ns = make_float2(-s0, -s1);
 }
 
+// ---------------------------------------------------------------------------------
+// Block-anchor phases as 64-bit fixed-point turns (a phase accumulator): the start
+// phase -d/lambda and the per-block increment -d*32*slope/c (both in turns) are reduced
+// to their fractional part in FP64 and scaled by 2^64, after which every block phase is
+// one exact modular 64-bit addition.  The angle handed to the hardware sine/cosine is the
+// accumulator's top 32 bits, i.e. a wrapped angle in [-pi, pi) with 2^-32-turn steps.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long turns_to_fixed(double t) {
+    const double kRound = 6755399441055744.0;  // 1.5 * 2^52: rint for |t| < 2^51
+    const double n = (t + kRound) - kRound;
+    const double f = t - n;                     // [-0.5, 0.5]
+    return (unsigned long long)__double2ll_rn(f * 18446744073709551616.0);
+}
+
+__device__ __forceinline__ void fixed_cis(unsigned long long ph, float &c, float &s) {
+    const float theta = (float)(int)(ph >> 32) * 1.46291807926715968e-9f;  // 2*pi / 2^32
+    __sincosf(theta, &s, &c);
+}
+
 // FP64 round-trip distance TX -> v -> RX.  `mono` (all RX offsets zero) reuses the
 // forward leg for the return leg, which is bit-identical to computing it again.
 __device__ __forceinline__ double range_fp64(double vx, double vy, double vz,

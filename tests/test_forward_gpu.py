@@ -147,7 +147,7 @@ def test_deterministic_and_status_clean(cuda_dev):
     assert ops.read_status(ws) == 0
 
 
-@pytest.mark.parametrize("idx", list(range(8)))
+@pytest.mark.parametrize("idx", list(range(12)))
 def test_every_mixed_variant(cuda_dev, oracle, idx):
     from mmnorm_b200 import ops
     n = len(ops.variants("mixed"))
@@ -225,19 +225,22 @@ def test_pair_and_scalar_mixed_forms_agree_bitwise(cuda_dev, n_ap):
     with a zero antenna by the antenna-pair form)."""
     from mmnorm_b200 import ops
     names = [v["name"] for v in ops.variants("mixed")]
-    picks = [names.index(n) for n in ("mixed_ffma_t4_n128", "mixed_ffma2_t4_n128",
-                                      "mixed_antpair_t2_n256", "mixed_antpair_t1_n256")]
+    groups = [("mixed_ffma_t4_n128", "mixed_ffma2_t4_n128", "mixed_antpair_t2_n256",
+               "mixed_antpair_t1_n256"),
+              ("mixed_ffma2_fx_t2_n256", "mixed_ffma2_fx_t4_n128", "mixed_antpair_fx_t2_n256",
+               "mixed_antpair_fx_t1_n256")]
     sc = scenes.sphere_scene(seed=16, n_ap=n_ap, nf=64, n_vox=11, n_pts=20)
-    out = []
-    for idx in picks:
-        ops.set_variant("mixed", idx)
-        try:
-            out.append(run_ops(cuda_dev, sc, "mixed"))
-        finally:
-            ops.set_variant("mixed", 0)
-    for o in out[1:]:
-        assert np.array_equal(out[0][0], o[0])
-        assert np.array_equal(out[0][1], o[1])
+    for group in groups:
+        out = []
+        for name in group:
+            ops.set_variant("mixed", names.index(name))
+            try:
+                out.append(run_ops(cuda_dev, sc, "mixed"))
+            finally:
+                ops.set_variant("mixed", 0)
+        for o in out[1:]:
+            assert np.array_equal(out[0][0], o[0])
+            assert np.array_equal(out[0][1], o[1])
 
 
 def test_autotuner_selects_a_variant(cuda_dev):
