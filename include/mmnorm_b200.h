@@ -99,6 +99,28 @@ int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vot
                     void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /*
+ * mmn_backproject without any device allocation (no counterpart in the reference, which
+ * allocates through pycuda on every call).  For callers that cannot call cudaMalloc
+ * where they image -- inside a stream capture, under a host that forbids allocation
+ * after start-up, in a real-time loop.  Same inputs, outputs and modes as
+ * mmn_backproject; the scratch comes from a 16 MiB device array built into the library,
+ * which every GPU that loads the library holds until the process exits.
+ *   - Limit: the antenna records plus the staged samples must fit 16 MiB (about
+ *     256 + 64*A + 16*A*roundup(F, 32) bytes in the default form, e.g. A*F up to about
+ *     one million antenna-samples); larger problems return MMN_ERR_TOO_LARGE before
+ *     anything runs.  Every voxel tile takes the whole antenna range (no antenna split),
+ *     so problems with few voxels run slower than through mmn_backproject.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call before any
+ *     stream capture.
+ *   - All calls share the one array per device and each call re-initialises what it
+ *     reads; calls whose work overlaps on the GPU (different streams, or host threads
+ *     without ordering) race on it and must be serialised by the caller.
+ */
+int mmn_backproject_noalloc(const mmn_problem *p, int32_t mode, float *image, float *vote,
+                            cudaStream_t stream);
+
+/*
  * Unit surface normals from (image, vote): mask |I| > filter_percent * max|I|
  * (src/data_processing/cuda/py_sn_est_gpu.py:326), raw normal Re(conj(I) W)/|I|
  * (surface_normal_est.cu:138-144), unit normalisation (image_processor.py:396).

@@ -12,6 +12,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "bp_kernels.cuh"
 
@@ -547,3 +548,71 @@ int mmn_read_status(void *workspace, int32_t *status, cudaStream_t stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// Backprojection that allocates nothing.
+//
+// Some callers cannot call cudaMalloc at the point where they image: code that runs
+// while a stream is being captured, hosts that hand their whole device pool to another
+// allocator and forbid allocation after start-up, and real-time loops that must not
+// block on the allocator.  mmn_backproject_noalloc serves them with a scratch area that
+// is part of the library image itself: a file-scope device array, allocated by the CUDA
+// runtime when the library's module is loaded on a device and held until the process
+// exits.  Its device address is looked up once per device (cudaGetSymbolAddress) on the
+// first call made with that device current.  The caller still owns inputs and outputs.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;  // 16 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  In host code the array's
+// name only stands in for the symbol, so the address has to come from the runtime.
+int noalloc_scratch(void **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return MMN_ERR_CUDA;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return MMN_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *addr = nullptr;
+        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr)
+            return MMN_ERR_CUDA;
+        g_noalloc_addr[dev] = addr;
+    }
+    *out = g_noalloc_addr[dev];
+    return MMN_OK;
+}
+
+}  // namespace
+
+extern "C" int mmn_backproject_noalloc(const mmn_problem *p, int32_t mode, float *image,
+                                       float *vote, cudaStream_t stream) {
+    int rc = check_problem(p, mode);
+    if (rc != MMN_OK) return rc;
+    if (!image) return MMN_ERR_NULL_POINTER;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    FwdPlan pl;
+    const bool full = mode != MMN_MODE_INTERP && p->num_antennas > 0;
+    if (full) {
+        rc = plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode,
+                          aligned16(p->meas), false, &pl);
+        if (rc != MMN_OK) return rc;
+        // every voxel tile takes the whole antenna range: no partial sums to hold
+        pl.splits = 1;
+        pl.ant_per_split = pl.a_pad;
+        pl.total = pl.off_partial;
+        if (pl.total > kNoAllocScratchBytes) return MMN_ERR_TOO_LARGE;
+    }
+    void *scratch = nullptr;
+    rc = noalloc_scratch(&scratch);
+    if (rc != MMN_OK) return rc;
+    if (!full)  // interpolated mode and empty apertures only need the status header
+        return mmn_backproject(p, mode, image, vote, scratch, kNoAllocScratchBytes, stream);
+    return run_forward(pl, p, nullptr, nullptr, reinterpret_cast<float2 *>(image),
+                       reinterpret_cast<float2 *>(vote), nullptr, nullptr,
+                       static_cast<unsigned char *>(scratch), stream);
+}

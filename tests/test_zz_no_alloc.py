@@ -1,0 +1,96 @@
+"""mmn_backproject_noalloc: the backprojection entry point for callers that cannot
+allocate device memory (stream capture, hosts that forbid allocation after start-up,
+real-time loops).  It must give the same image and vote as mmn_backproject, call after
+call, and refuse problems whose scratch would not fit its built-in 16 MiB array.
+
+This file is collected last on purpose: the entry point's first call on a device
+performs its one-time set-up, and the test must pass both in a fresh process and after
+every other test has run."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from mmnorm_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+TOL = 2e-5  # the mixed form's tolerance used throughout the forward tests
+
+
+def _tensors(dev, sc, meas=None, ant=None):
+    import torch
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    meas = sc.meas if meas is None else meas
+    ant = sc.antenna_locs if ant is None else ant
+    return [t(sc.x_locs), t(sc.y_locs), t(sc.z_locs), t(ant),
+            t(np.zeros((1, 3), np.float32)), t(meas)]
+
+
+def _noalloc(args, sc, mode, dev):
+    import torch
+    from mmnorm_b200 import _lib, ops
+    p = ops.make_problem(*args, sc.wavelength, sc.slope, fft_spacing=getattr(sc, "fsp", 0.0))
+    V = p.num_x * p.num_y * p.num_z
+    image = torch.empty(V, dtype=torch.complex64, device=dev)
+    vote = torch.empty((3, V), dtype=torch.complex64, device=dev)
+    rc = _lib.load().mmn_backproject_noalloc(ctypes.byref(p), _lib.MODES[mode], ops._vp(image),
+                                             ops._vp(vote), ops._stream(dev))
+    return rc, image, vote
+
+
+def _rel(a, b):
+    a = a.cpu().numpy().ravel()
+    b = b.cpu().numpy().ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("mode", ["mixed", "plain"])
+def test_noalloc_matches_backproject_twice(cuda_dev, mode):
+    import torch
+    from mmnorm_b200 import _lib, ops
+    sc = scenes.config0()  # 32x32 aperture, 64 frequencies, 48^3 voxels
+    args = _tensors(cuda_dev, sc)
+    ref_img, ref_vote = ops.backproject(*args, sc.wavelength, sc.slope, mode=mode)
+    firsts = None
+    for call in range(2):
+        rc, img, vote = _noalloc(args, sc, mode, cuda_dev)
+        assert rc == _lib.MMN_OK
+        torch.cuda.synchronize()
+        assert _rel(img, ref_img) < TOL, call
+        assert _rel(vote, ref_vote) < TOL, call
+        if firsts is None:
+            firsts = (img.clone(), vote.clone())
+        else:  # the shared scratch keeps no state that changes a later call's result
+            assert torch.equal(img, firsts[0]) and torch.equal(vote, firsts[1])
+
+
+def test_noalloc_interpolated_mode(cuda_dev):
+    import torch
+    from mmnorm_b200 import _lib, ops
+    sc = scenes.sphere_scene(seed=31, n_ap=12, nf=64, n_vox=10, n_pts=30, sign=+1)
+    pad = np.zeros((sc.meas.shape[0], 512), np.complex64)
+    pad[:, :64] = sc.meas
+    fft = np.fft.fft(pad, axis=1).astype(np.complex64)
+    sc.fsp = float(np.float32(3e8 / (2 * (sc.f_hi - sc.f_lo)) * 64 / 512))
+    args = _tensors(cuda_dev, sc, meas=fft)
+    ref_img, ref_vote = ops.backproject(*args, sc.wavelength, sc.slope, mode="interp",
+                                        fft_spacing=sc.fsp)
+    for _ in range(2):
+        rc, img, vote = _noalloc(args, sc, "interp", cuda_dev)
+        assert rc == _lib.MMN_OK
+        torch.cuda.synchronize()
+        assert torch.equal(img, ref_img.reshape(-1))
+        assert torch.equal(vote, ref_vote.reshape(3, -1))
+
+
+def test_noalloc_rejects_problems_beyond_its_scratch(cuda_dev):
+    from mmnorm_b200 import _lib
+    sc = scenes.sphere_scene(seed=32, n_ap=4, nf=16, n_vox=4, n_pts=5)
+    A, F = 8192, 256  # staged samples alone need 32 MiB > 16 MiB
+    meas = np.zeros((A, F), np.complex64)
+    ant = np.zeros((A, 3), np.float32)
+    ant[:, 2] = -0.1
+    args = _tensors(cuda_dev, sc, meas=meas, ant=ant)
+    rc, _, _ = _noalloc(args, sc, "mixed", cuda_dev)
+    assert rc == _lib.MMN_ERR_TOO_LARGE
