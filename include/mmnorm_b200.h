@@ -99,6 +99,20 @@ int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vot
                     void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /*
+ * Adjoint of mmn_backproject in MMN_MODE_MIXED (no counterpart in the reference, which
+ * has no gradients).  Given dL/dI (grad_image, complex64 [V]) and dL/dW (grad_vote,
+ * complex64 [3, V]; either may be NULL = zero) in the convention grad = dL/dRe + i dL/dIm,
+ * writes dL/dmeas (grad_meas, complex64 [num_antennas, num_samples], or NULL) and the
+ * gradient with respect to per-antenna position offsets added to TX and RX (grad_pos,
+ * float32 [num_antennas, 3], or NULL).  Phasors are recomputed; nothing per
+ * (voxel, antenna) is stored.  Needs mmn_backward_workspace_bytes() of workspace.
+ */
+size_t mmn_backward_workspace_bytes(const mmn_problem *p);
+int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
+                             const float *grad_vote, float *grad_meas, float *grad_pos,
+                             void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/*
  * mmn_backproject without any device allocation (no counterpart in the reference, which
  * allocates through pycuda on every call).  For callers that cannot call cudaMalloc
  * where they image -- inside a stream capture, under a host that forbids allocation

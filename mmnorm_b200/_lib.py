@@ -78,6 +78,8 @@ SIGNATURES = [
     ("mmn_plan_info", _I, [_PROB, _I32, _I32P, _I32P, _I32P, _I32P, _I32P]),
     ("mmn_backproject", _I, [_PROB, _I32, _P, _P, _P, _SZ, _P]),
     ("mmn_backproject_noalloc", _I, [_PROB, _I32, _P, _P, _P]),
+    ("mmn_backward_workspace_bytes", _SZ, [_PROB]),
+    ("mmn_backproject_backward", _I, [_PROB, _P, _P, _P, _P, _P, _SZ, _P]),
     ("mmn_normals_workspace_bytes", _SZ, [ctypes.c_int64]),
     ("mmn_normals", _I, [ctypes.c_int64, _P, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     ("mmn_cuda_image_workspace_bytes", _SZ, [_I, _I, _I]),

@@ -1,0 +1,334 @@
+// bp_backward.cu -- adjoint of the fused backprojection + vote (mixed precision).
+//
+// Forward (per voxel v, virtual antenna a, sample j):
+//   c_a(v) = sum_j m[a,j] p_aj(v),  p_aj = exp(-j d_a(v) kappa_j),  kappa_j = 2pi(1/lambda + j slope/c)
+//   I(v) = sum_a c_a(v),  W(v) = sum_a c_a(v) u_a(v),  u_a = tx_a + o_a/2 - v,
+//   with d_a(v) = |v - tx_a| + |v - rx_a| (+0.15), tx_a = antenna_a + delta_a, rx_a = tx_a + o_a.
+// Upstream gradients gI = dL/dI, gW = dL/dW in torch's convention (dL/dRe + i dL/dIm);
+// G_a(v) = gI(v) + sum_k gW_k(v) u_ak(v) is dL/dc_a(v).
+//
+//   dL/dm[a,j]   = sum_v G_a(v) conj(p_aj(v))                      (measurement pass)
+//   dL/ddelta_a  = sum_v [ Im(conj(G) c'_a) * (-(e_tx + e_rx)) + Re(conj(gW) c_a) ]
+//                  c'_a(v) = sum_j kappa_j m[a,j] p_aj(v),  e = unit vectors antenna -> voxel
+//                                                                  (position pass)
+// Phasors are recomputed, nothing per (voxel, antenna) is stored.
+//
+// Position pass: the forward's tiling and antenna staging; per (voxel, antenna) two Horner
+// chains ride in the two halves of every FFMA2 -- (kappa_j m_j) and (m_j), staged as
+// (kappa*re, re, kappa*im, im) -- with the forward's fixed-point block anchors.  Per-antenna
+// sums over a CTA's voxels (warp shuffles, then shared memory) go to per-tile partials
+// that a second kernel adds in tile order (deterministic).
+// Measurement pass: one thread per (antenna, 32-sample block); voxels stream through
+// shared memory; per voxel the block's 32 outputs receive G * conj(p) generated by an
+// FP32 rotation from an exact FP64-wrapped anchor (re-anchored per voxel and block).
+#include "bp_stage.cuh"
+
+namespace mmn {
+
+// (kappa_j re, re, kappa_j im, im) rows padded to Fp (antenna rows past A and samples past
+// F are zero).
+__global__ void bwd_stage_kernel(const float2 *__restrict__ meas, int A, int F, int Fp,
+                                 int rows, double k0, double kd, float4 *__restrict__ dst) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)rows * Fp) return;
+    const int64_t a = idx / Fp;
+    const int j = (int)(idx - a * Fp);
+    float2 m = make_float2(0.f, 0.f);
+    if (a < A && j < F) m = meas[a * F + j];
+    const float kap = (float)fma((double)j, kd, k0);
+    dst[idx] = make_float4(kap * m.x, m.x, kap * m.y, m.y);
+}
+
+__global__ void bwd_vox_rec_kernel(const BwdParams bp, float4 *__restrict__ dst) {
+    const FwdParams &p = bp.f;
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= p.nvox) return;
+    const int64_t nyz = (int64_t)p.ny * p.nz;
+    const int ix = (int)(v / nyz);
+    const int64_t rem = v - (int64_t)ix * nyz;
+    const int iy = (int)(rem / p.nz);
+    const int iz = (int)(rem - (int64_t)iy * p.nz);
+    const float2 gi = bp.grad_image ? bp.grad_image[v] : make_float2(0.f, 0.f);
+    float2 gw[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    if (bp.grad_vote)
+        for (int k = 0; k < 3; ++k) gw[k] = bp.grad_vote[k * p.nvox + v];
+    dst[3 * v + 0] = make_float4(p.x_locs[ix], p.y_locs[iy], p.z_locs[iz], 0.f);
+    dst[3 * v + 1] = make_float4(gi.x, gi.y, gw[0].x, gw[0].y);
+    dst[3 * v + 2] = make_float4(gw[1].x, gw[1].y, gw[2].x, gw[2].y);
+}
+
+// ------------------------------------------------------------------ position pass
+template <int T, int NT>
+__global__ void __launch_bounds__(NT) bp_bwd_pos_kernel(const BwdParams bp) {
+    const FwdParams &p = bp.f;
+    extern __shared__ __align__(128) unsigned char smem[];
+    Stage st;
+    st.bars = reinterpret_cast<uint64_t *>(smem);
+    st.base = smem + 128;
+    st.nas = p.ant_per_stage;
+    st.esz = 16;
+    st.fp = p.fp;
+    st.stage_bytes = (size_t)st.nas * sizeof(AntRec) + (size_t)st.nas * st.fp * st.esz;
+    float *wsum = reinterpret_cast<float *>(st.base + 2 * st.stage_bytes);  // [NT/32][nas][3]
+    constexpr int NW = NT / 32;
+    const int fp = p.fp;
+    const int tile = blockIdx.x % p.num_tiles;
+    const int split = blockIdx.x / p.num_tiles;
+    const int a_begin = split * p.ant_per_split;
+    const int a_end = min(p.num_ant, a_begin + p.ant_per_split);
+    const int n_chunks = a_end > a_begin ? (a_end - a_begin + st.nas - 1) / st.nas : 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        mbar_init(&st.bars[0], 1);
+        mbar_init(&st.bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n_chunks > 0) st.issue(p, 0, a_begin, a_end);
+        if (n_chunks > 1) st.issue(p, 1, a_begin, a_end);
+    }
+
+    const int64_t rbase = (int64_t)tile * (NT * T) + threadIdx.x;
+    float vx[T], vy[T], vz[T];
+    float2 gi[T], gw[T][3];
+#pragma unroll
+    for (int k = 0; k < T; ++k) {
+        const int64_t rel = rbase + (int64_t)k * NT;
+        decode_voxel(p, rel, vx[k], vy[k], vz[k]);
+        const bool ok = rel < p.vox_count;
+        const int64_t v = p.vox_start + (ok ? rel : 0);
+        gi[k] = (ok && bp.grad_image) ? bp.grad_image[v] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            gw[k][q] = (ok && bp.grad_vote) ? bp.grad_vote[q * p.nvox + v] : make_float2(0.f, 0.f);
+    }
+    const bool mono = *p.mono_flag != 0;
+    const int nblk = fp / kBlockF;
+
+    for (int c = 0; c < n_chunks; ++c) {
+        const int s = c & 1;
+        bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
+        if (!__syncthreads_and(ok)) return;
+        const AntRec *ants = st.ants(s);
+        const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
+        const int a0 = a_begin + c * st.nas;
+        const int na = min(st.nas, a_end - a0);
+
+        for (int a = 0; a < na; ++a) {
+            const AntRec &ar = ants[a];
+            const float4 *m4 = mstage + (size_t)a * fp;
+            float e3[T][3];
+            unsigned long long ph[T], stp[T];
+            float2 zr[T], zi[T], nzi[T], cr[T], ci[T];
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const double x = vx[k], y = vy[k], z = vz[k];
+                const double dx = x - ar.tx[0], dy = y - ar.tx[1], dz = z - ar.tx[2];
+                const double f = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+                double b = f, bx = dx, by = dy, bz = dz;
+                if (!mono) {
+                    bx = x - ar.rx[0];
+                    by = y - ar.rx[1];
+                    bz = z - ar.rx[2];
+                    b = sqrt(fma(bx, bx, fma(by, by, bz * bz)));
+                }
+                const double d = f + b + p.ti;
+                // -(e_tx + e_rx): derivative of d with respect to the antenna offset
+                e3[k][0] = -(float)(dx / f + bx / b);
+                e3[k][1] = -(float)(dy / f + by / b);
+                e3[k][2] = -(float)(dz / f + bz / b);
+                const float2 zz = cis_fp64_phase(-d * p.kd);
+                zr[k] = make_float2(zz.x, zz.x);
+                zi[k] = make_float2(zz.y, zz.y);
+                nzi[k] = make_float2(-zz.y, -zz.y);
+                ph[k] = turns_to_fixed(-d * p.t0);
+                stp[k] = turns_to_fixed(-d * p.tblk);
+                cr[k] = ci[k] = make_float2(0.f, 0.f);
+            }
+            for (int b = 0; b < nblk; ++b) {
+                const float4 *mb = m4 + b * kBlockF;
+                float2 hr[T], hi[T];
+                const float4 top = mb[kBlockF - 1];
+#pragma unroll
+                for (int k = 0; k < T; ++k) {
+                    hr[k] = make_float2(top.x, top.y);
+                    hi[k] = make_float2(top.z, top.w);
+                }
+#pragma unroll
+                for (int t = kBlockF - 2; t >= 0; --t) {
+                    const float4 mm = mb[t];
+                    const float2 mr = make_float2(mm.x, mm.y), mi = make_float2(mm.z, mm.w);
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        const float2 u = __ffma2_rn(hr[k], zr[k], mr);
+                        const float2 w = __ffma2_rn(hr[k], zi[k], mi);
+                        hr[k] = __ffma2_rn(hi[k], nzi[k], u);
+                        hi[k] = __ffma2_rn(hi[k], zr[k], w);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < T; ++k) {
+                    float ac, as;
+                    fixed_cis(ph[k], ac, as);
+                    ph[k] += stp[k];
+                    const float2 anr = make_float2(ac, ac), ani = make_float2(as, as),
+                                 nani = make_float2(-as, -as);
+                    cr[k] = __ffma2_rn(anr, hr[k], __ffma2_rn(nani, hi[k], cr[k]));
+                    ci[k] = __ffma2_rn(anr, hi[k], __ffma2_rn(ani, hr[k], ci[k]));
+                }
+            }
+            // lane .x carries c' = sum kappa m p, lane .y carries c = sum m p
+            float g3[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const float u[3] = {ar.virt[0] - vx[k], ar.virt[1] - vy[k], ar.virt[2] - vz[k]};
+                float Gr = gi[k].x, Gi = gi[k].y;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    Gr = fmaf(gw[k][q].x, u[q], Gr);
+                    Gi = fmaf(gw[k][q].y, u[q], Gi);
+                }
+                const float s1 = Gr * ci[k].x - Gi * cr[k].x;  // Im(conj(G) c')
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+                    g3[q] += fmaf(s1, e3[k][q], gw[k][q].x * cr[k].y + gw[k][q].y * ci[k].y);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) g3[q] += __shfl_xor_sync(0xffffffffu, g3[q], o);
+            }
+            if (lane == 0) {
+                wsum[(warp * st.nas + a) * 3 + 0] = g3[0];
+                wsum[(warp * st.nas + a) * 3 + 1] = g3[1];
+                wsum[(warp * st.nas + a) * 3 + 2] = g3[2];
+            }
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < na * 3; idx += NT) {
+            float sum = 0.f;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) sum += wsum[w * st.nas * 3 + idx];
+            bp.pos_partial[((size_t)tile * p.num_ant + a0) * 3 + idx] = sum;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
+    }
+}
+
+__global__ void bwd_pos_reduce_kernel(const BwdParams bp) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= bp.num_ant_real * 3) return;
+    float s = 0.f;
+    for (int t = 0; t < bp.f.num_tiles; ++t)
+        s += bp.pos_partial[(size_t)t * bp.f.num_ant * 3 + idx];
+    bp.grad_pos[idx] = s;
+}
+
+// --------------------------------------------------------------- measurement pass
+constexpr int kMeasThreads = 128;
+constexpr int kVoxChunk = 256;  // voxel records per shared-memory chunk (12 KB)
+
+__global__ void __launch_bounds__(kMeasThreads) bp_bwd_meas_kernel(const BwdParams bp) {
+    const FwdParams &p = bp.f;
+    __shared__ float4 vrec[kVoxChunk * 3];
+    const int nblk = p.fp / kBlockF;
+    const int item = blockIdx.x * kMeasThreads + threadIdx.x;
+    const bool active = item < bp.num_items;
+    const int it = active ? item : 0;
+    const int a = it / nblk;
+    const int b = it - a * nblk;
+    const AntRec ar = p.ant[a];
+    const bool mono = *p.mono_flag != 0;
+    const double kap = fma((double)(b * kBlockF), p.kd, p.k0);
+    float accr[kBlockF], acci[kBlockF];
+#pragma unroll
+    for (int t = 0; t < kBlockF; ++t) accr[t] = acci[t] = 0.f;
+
+    for (int64_t v0 = 0; v0 < p.nvox; v0 += kVoxChunk) {
+        const int nv = (int)min((int64_t)kVoxChunk, p.nvox - v0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nv * 3; q += kMeasThreads) vrec[q] = bp.vox_rec[v0 * 3 + q];
+        __syncthreads();
+        if (!active) continue;
+        for (int j = 0; j < nv; ++j) {
+            const float4 r0 = vrec[3 * j], r1 = vrec[3 * j + 1], r2 = vrec[3 * j + 2];
+            const double d = range_fp64((double)r0.x, (double)r0.y, (double)r0.z, ar, mono, p.ti);
+            const float2 z = cis_fp64_phase(d * p.kd);   // conj of the forward step
+            const float2 an = cis_fp64_phase(d * kap);   // conj of the forward block anchor
+            const float ux = ar.virt[0] - r0.x, uy = ar.virt[1] - r0.y, uz = ar.virt[2] - r0.z;
+            const float Gr = fmaf(r2.z, uz, fmaf(r2.x, uy, fmaf(r1.z, ux, r1.x)));
+            const float Gi = fmaf(r2.w, uz, fmaf(r2.y, uy, fmaf(r1.w, ux, r1.y)));
+            float qr = Gr * an.x - Gi * an.y;
+            float qi = Gr * an.y + Gi * an.x;
+#pragma unroll
+            for (int t = 0; t < kBlockF; ++t) {
+                accr[t] += qr;
+                acci[t] += qi;
+                const float nr = fmaf(qr, z.x, -qi * z.y);
+                qi = fmaf(qr, z.y, qi * z.x);
+                qr = nr;
+            }
+        }
+    }
+    if (!active) return;
+#pragma unroll
+    for (int t = 0; t < kBlockF; ++t) {
+        const int j = b * kBlockF + t;
+        if (j < bp.num_samples) bp.grad_meas[(size_t)a * bp.num_samples + j] = make_float2(accr[t], acci[t]);
+    }
+}
+
+// -------------------------------------------------------------------- launchers
+const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread) {
+    if (variant == 1) {
+        *threads = 128;
+        *voxels_per_thread = 2;
+        return reinterpret_cast<const void *>(&bp_bwd_pos_kernel<2, 128>);
+    }
+    *threads = 256;
+    *voxels_per_thread = 1;
+    return reinterpret_cast<const void *>(&bp_bwd_pos_kernel<1, 256>);
+}
+
+cudaError_t launch_bwd_stage(const float *meas, int A, int F, int Fp, double k0, double kd,
+                             void *dst, cudaStream_t stream) {
+    const int nt = 256;
+    const int rows = A;
+    const int64_t n = (int64_t)rows * Fp;
+    bwd_stage_kernel<<<(unsigned)((n + nt - 1) / nt), nt, 0, stream>>>(
+        reinterpret_cast<const float2 *>(meas), A, F, Fp, rows, k0, kd,
+        reinterpret_cast<float4 *>(dst));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bwd_vox_rec(const BwdParams &bp, float4 *dst, cudaStream_t stream) {
+    const int nt = 256;
+    bwd_vox_rec_kernel<<<(unsigned)((bp.f.nvox + nt - 1) / nt), nt, 0, stream>>>(bp, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bwd_pos(const BwdParams &bp, int variant, size_t smem, cudaStream_t stream) {
+    int nt = 0, t = 0;
+    const void *fn = bwd_pos_kernel_ptr(variant, &nt, &t);
+    void *args[] = {const_cast<BwdParams *>(&bp)};
+    return cudaLaunchKernel(fn, dim3(bp.f.num_tiles * bp.f.num_splits), dim3(nt), args, smem,
+                            stream);
+}
+
+cudaError_t launch_bwd_pos_reduce(const BwdParams &bp, cudaStream_t stream) {
+    const int nt = 256;
+    const int n = bp.num_ant_real * 3;
+    bwd_pos_reduce_kernel<<<(n + nt - 1) / nt, nt, 0, stream>>>(bp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bwd_meas(const BwdParams &bp, cudaStream_t stream) {
+    const int blocks = (bp.num_items + kMeasThreads - 1) / kMeasThreads;
+    bp_bwd_meas_kernel<<<blocks, kMeasThreads, 0, stream>>>(bp);
+    return cudaGetLastError();
+}
+
+}  // namespace mmn

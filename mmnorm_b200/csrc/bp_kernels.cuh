@@ -53,6 +53,29 @@ cudaError_t launch_prep_antennas(const float *ant, const float *rxo, int R, cons
 cudaError_t launch_stage_meas(const float *src, const float *im, int A, int F, int Fp,
                               int layout, void *dst, cudaStream_t stream);
 
+// ------------------------------------------------------------------- backward
+struct BwdParams {
+    FwdParams f;               // geometry, antenna records, staged (kappa*m, m) samples, tiles
+    const float2 *grad_image;  // [nvox] complex64 dL/dI (torch convention)
+    const float2 *grad_vote;   // [3, nvox] complex64 dL/dW, or null
+    float *pos_partial;        // [num_tiles, a_pad, 3] per-tile position-gradient sums
+    const float4 *vox_rec;     // [nvox, 3] voxel records (x, y, z, -), (gI, gWx), (gWy, gWz)
+    float2 *grad_meas;         // [num_ant_real, num_samples] complex64
+    float *grad_pos;           // [num_ant_real, 3]
+    int32_t num_samples;       // unpadded F
+    int32_t num_ant_real;      // A before padding
+    int32_t num_items;         // num_ant_real * (fp / 32): (antenna, 32-sample block) pairs
+    int32_t pad0;
+};
+
+cudaError_t launch_bwd_stage(const float *meas, int A, int F, int Fp, double k0, double kd,
+                             void *dst, cudaStream_t stream);
+cudaError_t launch_bwd_vox_rec(const BwdParams &bp, float4 *dst, cudaStream_t stream);
+cudaError_t launch_bwd_pos(const BwdParams &bp, int variant, size_t smem, cudaStream_t stream);
+cudaError_t launch_bwd_pos_reduce(const BwdParams &bp, cudaStream_t stream);
+cudaError_t launch_bwd_meas(const BwdParams &bp, cudaStream_t stream);
+const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread);
+
 // ---------------------------------------------------------- interpolated mode
 struct InterpParams {
     const float *x_locs, *y_locs, *z_locs;

@@ -550,6 +550,162 @@ int mmn_read_status(void *workspace, int32_t *status, cudaStream_t stream) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------
+// Backward pass (adjoint) of the mixed-precision fused backprojection.
+// ---------------------------------------------------------------------------------
+namespace {
+
+std::atomic<int> g_bwd_variant{0};
+
+struct BwdPlan {
+    int fp, ant_per_stage, tiles, splits, ant_per_split, threads, vpt;
+    size_t smem;
+    size_t off_ant, off_meas, off_vox, off_pos, total;
+    const void *fn;
+};
+
+int plan_backward(const mmn_problem *p, BwdPlan *pl) {
+    const int A = p->num_antennas;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    pl->fn = bwd_pos_kernel_ptr(g_bwd_variant.load(), &pl->threads, &pl->vpt);
+    pl->fp = (p->num_samples + kBlockF - 1) / kBlockF * kBlockF;
+    if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
+    const int rec = (int)sizeof(AntRec) + pl->fp * 16;
+    pl->ant_per_stage = std::max(1, std::min(16, kMaxStageBytes / rec));
+    pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec +
+               (size_t)(pl->threads / 32) * pl->ant_per_stage * 3 * sizeof(float);
+    const int64_t per_tile = (int64_t)pl->threads * pl->vpt;
+    const int64_t tiles = (nvox + per_tile - 1) / per_tile;
+    if (tiles > (int64_t)1 << 30) return MMN_ERR_TOO_LARGE;
+    pl->tiles = (int)std::max<int64_t>(1, tiles);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (pl->smem > 48 * 1024)
+        cudaFuncSetAttribute(pl->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->fn, pl->threads, pl->smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int64_t slots = (int64_t)sms * per_sm;
+    int best_s = 1;
+    double best_cost = 1e300;
+    const int max_s = std::max(1, std::min(64, (A + pl->ant_per_stage - 1) / pl->ant_per_stage));
+    for (int s = 1; s <= max_s; ++s) {
+        const int64_t ctas = (int64_t)pl->tiles * s;
+        const double waves = (double)((ctas + slots - 1) / slots);
+        const double cost = waves * std::ceil((double)A / s) * (1.0 + 0.02 * (s - 1));
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best_s = s;
+        }
+        if (ctas >= 8 * slots) break;
+    }
+    int aps = (A + best_s - 1) / best_s;
+    aps = (aps + pl->ant_per_stage - 1) / pl->ant_per_stage * pl->ant_per_stage;
+    pl->ant_per_split = std::max(aps, 1);
+    pl->splits = std::max(1, (A + pl->ant_per_split - 1) / pl->ant_per_split);
+    size_t off = kStatusBytes;
+    pl->off_ant = off;
+    off = align_up(off + (size_t)A * sizeof(AntRec));
+    pl->off_meas = off;
+    off = align_up(off + (size_t)A * pl->fp * 16);
+    pl->off_vox = off;
+    off = align_up(off + (size_t)nvox * 3 * sizeof(float4));
+    pl->off_pos = off;
+    off = align_up(off + (size_t)pl->tiles * A * 3 * sizeof(float));
+    pl->total = off;
+    return MMN_OK;
+}
+
+}  // namespace
+
+extern "C" size_t mmn_backward_workspace_bytes(const mmn_problem *p) {
+    if (check_problem(p, MMN_MODE_MIXED) != MMN_OK) return 0;
+    BwdPlan pl;
+    if (plan_backward(p, &pl) != MMN_OK) return 0;
+    return pl.total;
+}
+
+extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
+                                        const float *grad_vote, float *grad_meas,
+                                        float *grad_pos, void *workspace,
+                                        size_t workspace_bytes, cudaStream_t stream) {
+    int rc = check_problem(p, MMN_MODE_MIXED);
+    if (rc != MMN_OK) return rc;
+    if (!grad_meas && !grad_pos) return MMN_ERR_NULL_POINTER;
+    if (!grad_image && !grad_vote) return MMN_ERR_NULL_POINTER;
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
+        return MMN_ERR_WORKSPACE;
+    const int A = p->num_antennas;
+    const int F = p->num_samples;
+    if (A == 0) return MMN_OK;
+    BwdPlan pl;
+    rc = plan_backward(p, &pl);
+    if (rc != MMN_OK) return rc;
+    if (workspace_bytes < pl.total) return MMN_ERR_WORKSPACE;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (cudaMemsetAsync(ws, 0, 16, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    AntRec *ant = reinterpret_cast<AntRec *>(ws + pl.off_ant);
+    int32_t *hdr = reinterpret_cast<int32_t *>(ws);
+    if (launch_prep_antennas(p->antenna_locs, p->rx_offsets, p->num_rx, p->pos_offsets, A, A, ant,
+                             hdr + 1, stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    BwdParams bp;
+    std::memset(&bp, 0, sizeof(bp));
+    FwdParams &f = bp.f;
+    f.x_locs = p->x_locs;
+    f.y_locs = p->y_locs;
+    f.z_locs = p->z_locs;
+    f.nx = p->num_x;
+    f.ny = p->num_y;
+    f.nz = p->num_z;
+    f.nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    f.vox_start = 0;
+    f.vox_count = f.nvox;
+    f.ant = ant;
+    f.meas = ws + pl.off_meas;
+    f.num_ant = A;
+    f.fp = pl.fp;
+    f.ant_per_stage = pl.ant_per_stage;
+    f.mono_flag = hdr + 1;
+    f.k0 = 2.0 * kPi / p->wavelength;
+    f.kd = 2.0 * kPi * p->slope / kC;
+    f.t0 = 1.0 / p->wavelength;
+    f.tblk = (double)kBlockF * p->slope / kC;
+    f.ti = p->is_ti_radar ? 0.15 : 0.0;
+    f.num_tiles = pl.tiles;
+    f.num_splits = pl.splits;
+    f.ant_per_split = pl.ant_per_split;
+    f.status = hdr;
+    bp.grad_image = reinterpret_cast<const float2 *>(grad_image);
+    bp.grad_vote = reinterpret_cast<const float2 *>(grad_vote);
+    bp.pos_partial = reinterpret_cast<float *>(ws + pl.off_pos);
+    bp.vox_rec = reinterpret_cast<const float4 *>(ws + pl.off_vox);
+    bp.grad_meas = reinterpret_cast<float2 *>(grad_meas);
+    bp.grad_pos = grad_pos;
+    bp.num_samples = F;
+    bp.num_ant_real = A;
+    bp.num_items = A * (pl.fp / kBlockF);
+    if (grad_pos) {
+        if (launch_bwd_stage(p->meas, A, F, pl.fp, f.k0, f.kd, ws + pl.off_meas, stream) !=
+            cudaSuccess)
+            return MMN_ERR_CUDA;
+        if (pl.smem > 48 * 1024)
+            cudaFuncSetAttribute(pl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+        if (launch_bwd_pos(bp, g_bwd_variant.load(), pl.smem, stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+        if (launch_bwd_pos_reduce(bp, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    }
+    if (grad_meas) {
+        if (launch_bwd_vox_rec(bp, reinterpret_cast<float4 *>(ws + pl.off_vox), stream) !=
+            cudaSuccess)
+            return MMN_ERR_CUDA;
+        if (launch_bwd_meas(bp, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    }
+    return MMN_OK;
+}
+
+// ---------------------------------------------------------------------------------
 // Backprojection that allocates nothing.
 //
 // Some callers cannot call cudaMalloc at the point where they image: code that runs

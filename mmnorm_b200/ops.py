@@ -170,3 +170,79 @@ def variants(mode="mixed"):
 
 def set_variant(mode, index):
     _lib.check(_lib.load().mmn_set_variant(_lib.MODES[mode], int(index)), "mmn_set_variant")
+
+
+def backproject_backward(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength,
+                         slope, grad_image, grad_vote, *, is_ti_radar=False, pos_offsets=None,
+                         want_meas=True, want_pos=True):
+    """Adjoint of the mixed-precision ``backproject``: (grad_meas complex64 [A, F] or None,
+    grad_pos float32 [A, 3] or None) for upstream dL/dI, dL/dW (torch convention)."""
+    p = make_problem(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
+                     0.0, is_ti_radar, pos_offsets)
+    dev = meas.device
+    V = p.num_x * p.num_y * p.num_z
+    gI = grad_image.reshape(V).contiguous() if grad_image is not None else None
+    gW = grad_vote.reshape(3, V).contiguous() if grad_vote is not None else None
+    if gI is None and gW is None:
+        gI = torch.zeros(V, dtype=torch.complex64, device=dev)
+    A, F = meas.shape
+    gm = torch.empty((A, F), dtype=torch.complex64, device=dev) if want_meas else None
+    gp = torch.empty((A, 3), dtype=torch.float32, device=dev) if want_pos else None
+    lib = _lib.load()
+    nbytes = lib.mmn_backward_workspace_bytes(ctypes.byref(p))
+    if nbytes == 0:
+        raise _lib.MmnError(_lib.MMN_ERR_INVALID_ARGUMENT, "mmn_backward_workspace_bytes")
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    rc = lib.mmn_backproject_backward(ctypes.byref(p), _vp(gI), _vp(gW), _vp(gm), _vp(gp),
+                                      _vp(ws), nbytes, _stream(dev))
+    _lib.check(rc, "mmn_backproject_backward")
+    return gm, gp
+
+
+class BackprojectFunction(torch.autograd.Function):
+    """Differentiable fused backprojection + vote (mixed precision).
+
+    Inputs differentiated: ``meas`` (complex64 [A, F]) and ``pos_offsets`` (float32
+    [A, 3], added to every TX and RX position: trajectory calibration).  The backward runs
+    the library's adjoint kernels; phasors are recomputed, not stored."""
+
+    @staticmethod
+    def forward(ctx, meas, pos_offsets, x_locs, y_locs, z_locs, antenna_locs, rx_offsets,
+                wavelength, slope, is_ti_radar):
+        image, vote = backproject(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas,
+                                  wavelength, slope, mode="mixed", is_ti_radar=is_ti_radar,
+                                  pos_offsets=pos_offsets)
+        ctx.save_for_backward(meas, pos_offsets, x_locs, y_locs, z_locs, antenna_locs,
+                              rx_offsets)
+        ctx.consts = (wavelength, slope, is_ti_radar)
+        return image, vote
+
+    @staticmethod
+    def backward(ctx, grad_image, grad_vote):
+        meas, pos, x, y, z, ant, rxo = ctx.saved_tensors
+        wavelength, slope, ti = ctx.consts
+        gm, gp = backproject_backward(
+            x, y, z, ant, rxo, meas, wavelength, slope,
+            grad_image.contiguous() if grad_image is not None else None,
+            grad_vote.contiguous() if grad_vote is not None else None,
+            is_ti_radar=ti, pos_offsets=pos, want_meas=ctx.needs_input_grad[0],
+            want_pos=ctx.needs_input_grad[1])
+        return gm, gp, None, None, None, None, None, None, None, None
+
+
+def backproject_differentiable(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas,
+                               wavelength, slope, pos_offsets=None, is_ti_radar=False):
+    """(image, vote) with autograd to ``meas`` and ``pos_offsets``."""
+    if pos_offsets is None:
+        pos_offsets = torch.zeros_like(antenna_locs)
+    return BackprojectFunction.apply(meas, pos_offsets, x_locs, y_locs, z_locs, antenna_locs,
+                                     rx_offsets, float(wavelength), float(slope),
+                                     bool(is_ti_radar))
+
+
+def normals_differentiable(image, vote, eps=1e-30):
+    """Unit normals from (image, vote) in torch ops (differentiable), no mask:
+    n = Re(conj(I) W)/|I| normalised (surface_normal_est.cu:138-144, image_processor.py:396)."""
+    mag = image.abs().clamp_min(eps)
+    raw = (image.conj().unsqueeze(0) * vote).real / mag.unsqueeze(0)
+    return raw / raw.norm(dim=0, keepdim=True).clamp_min(eps)
