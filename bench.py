@@ -46,6 +46,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU seconds of the bounded reference/CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--variant", default=None,
                     help="force a mixed kernel variant by name instead of autotuning")
     ap.add_argument("--aperture", type=int, default=128,
@@ -334,6 +335,10 @@ def ours_arm(args):
                         "mixed_over_plain": value / pval,
                         "variant": ops.variants("plain")[ptuned["best"]]["name"]}
 
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = time_adjoint(dev)
+
     # end to end through the public API: pinned host inputs -> device -> image + normals
     # -> pinned host outputs, every step
     e2e = None
@@ -420,6 +425,7 @@ def ours_arm(args):
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "cpu_baseline": cpu,
+            "adjoint": adjoint,
         }
         line.update(out)
         print(json.dumps(line))
@@ -427,6 +433,48 @@ def ours_arm(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def time_adjoint(dev):
+    """Forward vs backward cost on the differentiation workload (64^3 voxels @3 mm,
+    64x64 antennas @3 mm, 128 frequencies, sphere scene): device time of the fused
+    forward (image + vote) and of the adjoint (measurement + position gradients)."""
+    import torch
+    from mmnorm_b200 import ops, scenes
+    sc = scenes.config3(sign=+1, device=dev)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    args = [t(sc.x_locs), t(sc.y_locs), t(sc.z_locs), t(sc.antenna_locs),
+            t(np.zeros((1, 3), np.float32)), t(sc.meas)]
+    rng = np.random.default_rng(3)
+    pos = t(rng.normal(0, 5e-4, sc.antenna_locs.shape).astype(np.float32))
+    V = sc.num_voxels
+    gI = t((rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64))
+    gW = t((rng.standard_normal((3, V)) + 1j * rng.standard_normal((3, V))).astype(np.complex64))
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    fwd = timed(lambda: ops.backproject(*args, sc.wavelength, sc.slope, pos_offsets=pos))
+    bwd = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
+                                                 pos_offsets=pos))
+    bwd_m = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
+                                                   pos_offsets=pos, want_pos=False))
+    bwd_p = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
+                                                   pos_offsets=pos, want_meas=False))
+    return {"workload": sc.name + " (64^3 voxels @3 mm, 64x64 antennas @3 mm, 128 freqs)",
+            "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+            "backward_meas_ms": bwd_m, "backward_pos_ms": bwd_p}
 
 
 def _read_traffic():

@@ -1,0 +1,86 @@
+"""Accuracy report of the mixed and the plain forms against the FP64 oracle:
+
+  * the 128^3-voxel, 128x128-antenna, 256-frequency workload (config 1 inputs) on a
+    seeded random 4096-voxel subset;
+  * a full 64^3 grid with config 0's aperture (32x32 @3 mm), 64 frequencies and 4 mm
+    spacing.
+
+Reported per form: complex-image relative L2 error, vote relative L2 error, median and
+95th-percentile normal angle (degrees) over the masked voxels (mask |I| > 5 % of the
+image maximum).  Targets asserted for the mixed form: <= 1e-4 relative L2 and <= 0.5 deg
+median normal error.  If MMN_REPORT_DIR is set the numbers are written there as JSON."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from mmnorm_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(dev, sc, mode):
+    import torch
+    from mmnorm_b200 import ops
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    img, vote = ops.backproject(t(sc.x_locs), t(sc.y_locs), t(sc.z_locs), t(sc.antenna_locs),
+                                t(np.zeros((1, 3), np.float32)), t(sc.meas), sc.wavelength,
+                                sc.slope, mode=mode)
+    torch.cuda.synchronize()
+    return img.cpu().numpy().ravel(), vote.cpu().numpy().reshape(3, -1).T
+
+
+def _stats(oracle, I, W, idx, Io, Wo):
+    mag_full = np.abs(I)
+    thr = 0.05 * mag_full.max()
+    sel = np.abs(Io) > thr
+    _, _, raw_o = oracle.normals_from_vote(Io, Wo, 0.0)
+    _, _, raw = oracle.normals_from_vote(I[idx].astype(np.complex128),
+                                         W[idx].astype(np.complex128), 0.0)
+    ang = oracle.angle_deg(raw[sel], raw_o[sel])
+    return {"image_rel_l2": oracle.rel_l2(I[idx], Io), "vote_rel_l2": oracle.rel_l2(W[idx], Wo),
+            "normal_deg_median": float(np.median(ang)) if ang.size else None,
+            "normal_deg_p95": float(np.percentile(ang, 95)) if ang.size else None,
+            "masked_voxels": int(sel.sum()), "voxels": int(len(idx))}
+
+
+def _report(name, data):
+    d = os.environ.get("MMN_REPORT_DIR")
+    if d:
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, name + ".json"), "w") as f:
+            json.dump(data, f, indent=1)
+    print(name, json.dumps(data))
+
+
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_accuracy_workload_subset(cuda_dev, oracle, sign):
+    sc = scenes.config1(sign=sign, device=cuda_dev)
+    rng = np.random.default_rng(2)
+    idx = np.sort(rng.choice(sc.num_voxels, 4096, replace=False))
+    Io, Wo = oracle.full(sc.voxel_centres(idx), sc.antenna_locs, np.zeros((1, 3)), sc.meas,
+                         sc.wavelength, sc.slope, phase_mode=1)
+    out = {"workload": sc.name, "sign": sign, "subset": "4096 seeded random voxels"}
+    for mode in ("mixed", "plain"):
+        I, W = _run(cuda_dev, sc, mode)
+        out[mode] = _stats(oracle, I, W, idx, Io, Wo)
+    _report("accuracy_%s_sign%+d" % (sc.name, sign), out)
+    assert out["mixed"]["image_rel_l2"] <= 1e-4
+    assert out["mixed"]["vote_rel_l2"] <= 1e-4
+    assert out["mixed"]["normal_deg_median"] <= 0.5
+
+
+def test_accuracy_full_grid_64(cuda_dev, oracle):
+    sc = scenes.sphere_scene(seed=0, n_ap=32, pitch=3e-3, nf=64, n_vox=64, spacing=4e-3,
+                             name="sphere64_ap32_f64")
+    idx = np.arange(sc.num_voxels)
+    Io, Wo = oracle.full(sc.voxel_centres(), sc.antenna_locs, np.zeros((1, 3)), sc.meas,
+                         sc.wavelength, sc.slope, phase_mode=1)
+    out = {"workload": sc.name, "sign": -1, "subset": "full 64^3 grid"}
+    for mode in ("mixed", "plain"):
+        I, W = _run(cuda_dev, sc, mode)
+        out[mode] = _stats(oracle, I, W, idx, Io, Wo)
+    _report("accuracy_" + sc.name, out)
+    assert out["mixed"]["image_rel_l2"] <= 1e-4
+    assert out["mixed"]["normal_deg_median"] <= 0.5
