@@ -47,6 +47,7 @@ def parse_args():
                     help="target CPU seconds of the bounded reference/CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--variant", default=None,
                     help="force a mixed kernel variant by name instead of autotuning")
     ap.add_argument("--aperture", type=int, default=128,
@@ -338,6 +339,9 @@ def ours_arm(args):
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = time_adjoint(dev)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = time_batched(dev)
 
     # end to end through the public API: pinned host inputs -> device -> image + normals
     # -> pinned host outputs, every step
@@ -426,6 +430,7 @@ def ours_arm(args):
             "gpu_launches": launches_per_step * args.steps,
             "cpu_baseline": cpu,
             "adjoint": adjoint,
+            "batched": batched,
         }
         line.update(out)
         print(json.dumps(line))
@@ -475,6 +480,52 @@ def time_adjoint(dev):
     return {"workload": sc.name + " (64^3 voxels @3 mm, 64x64 antennas @3 mm, 128 freqs)",
             "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
             "backward_meas_ms": bwd_m, "backward_pos_ms": bwd_p}
+
+
+def time_batched(dev, replays=3):
+    """24 uneven objects (grids 32^3-96^3, apertures 32^2-96^2 at 2-4 mm, 64-256
+    frequencies) in one persistent, graph-captured launch: aggregate updates/s, the same
+    objects launched one by one, and the worst per-object deviation between the two."""
+    import torch
+    from mmnorm_b200 import autotune, ops, scenes
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    scs = scenes.config4_objects(sign=-1, device=dev)
+    objs = [dict(x_locs=t(sc.x_locs), y_locs=t(sc.y_locs), z_locs=t(sc.z_locs),
+                 antenna_locs=t(sc.antenna_locs), rx_offsets=t(np.zeros((1, 3), np.float32)),
+                 meas=t(sc.meas), wavelength=sc.wavelength, slope=sc.slope) for sc in scs]
+    updates = sum(sc.updates for sc in scs)
+    tuned = autotune.tune_batched(objs)
+    plan = ops.BatchPlan(objs, items_per_slot=tuned["best"])
+    plan.capture()
+    plan.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(replays):
+        plan.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / replays
+    # one by one, same kernels, for the comparison and the per-object check
+    worst = 0.0
+    i0, i1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    i0.record()
+    singles = [ops.backproject(o["x_locs"], o["y_locs"], o["z_locs"], o["antenna_locs"],
+                               o["rx_offsets"], o["meas"], o["wavelength"], o["slope"])
+               for o in objs]
+    i1.record()
+    torch.cuda.synchronize()
+    ms_single = i0.elapsed_time(i1)
+    for (img, vote), (si, sv) in zip(plan.results(), singles):
+        for a, b in ((img, si), (vote, sv)):
+            worst = max(worst, float((a - b).abs().norm() / b.abs().norm()))
+    info = plan.info()
+    return {"objects": len(objs), "updates": updates, "ms": ms,
+            "value": updates / (ms * 1e-3) / 1e9, "unit": UNIT,
+            "one_by_one_ms": ms_single, "one_by_one_value": updates / (ms_single * 1e-3) / 1e9,
+            "max_rel_l2_vs_one_by_one": worst, "items": info["items"], "ctas": info["ctas"],
+            "items_per_slot": tuned["best"], "autotune_ms": tuned["times_ms"],
+            "graph": "captured once, replayed"}
 
 
 def _read_traffic():

@@ -113,6 +113,32 @@ int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
                              void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /*
+ * Batched persistent launch (no counterpart in the reference, which images one object per
+ * call; mmwave_reconstruction.sh:61-69 loops over objects in the shell).  Many objects --
+ * each its own voxel grid, aperture, sample count and radar constants -- run in ONE
+ * persistent kernel launch over a work list of (object, voxel tile, antenna split) items
+ * sorted by cost, largest first; CTAs pop items from a global counter.  MMN_MODE_MIXED only.
+ *   mmn_batch_create: plans the work list (about items_per_slot items per resident CTA;
+ *     <= 0 picks 8) for the given problems and output buffers (images[o]: complex64 [V_o];
+ *     votes[o]: complex64 [3, V_o] or NULL; votes itself may be NULL); returns the
+ *     workspace size.  Host-side only.
+ *   mmn_batch_upload: writes the plan's tables into the workspace (synchronises `stream`).
+ *   mmn_batch_run: per-object preparation kernels, the persistent kernel and the split
+ *     reductions -- only kernel launches and memsets, so it can be captured in a CUDA graph.
+ * Each object's result equals mmn_backproject's up to summation order across antenna splits.
+ */
+typedef struct mmn_batch mmn_batch;
+int mmn_batch_create(const mmn_problem *problems, int32_t num_objects, int32_t mode,
+                     float *const *images, float *const *votes, int32_t items_per_slot,
+                     mmn_batch **batch, size_t *workspace_bytes);
+int mmn_batch_upload(mmn_batch *batch, void *workspace, size_t workspace_bytes,
+                     cudaStream_t stream);
+int mmn_batch_run(mmn_batch *batch, void *workspace, cudaStream_t stream);
+int mmn_batch_info(const mmn_batch *batch, int32_t *num_items, int32_t *ctas, int32_t *threads,
+                   int32_t *voxels_per_thread);
+void mmn_batch_destroy(mmn_batch *batch);
+
+/*
  * mmn_backproject without any device allocation (no counterpart in the reference, which
  * allocates through pycuda on every call).  For callers that cannot call cudaMalloc
  * where they image -- inside a stream capture, under a host that forbids allocation

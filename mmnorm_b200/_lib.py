@@ -90,6 +90,12 @@ SIGNATURES = [
     ("mmn_cuda_sn_est", _I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _F,
                              _F, _F, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _SZ, _P]),
     ("mmn_fp32_peak_probe", _I, [_I, _I, _P, _P]),
+    ("mmn_batch_create", _I, [_PROB, _I32, _I32, _P, _P, _I32, ctypes.POINTER(_P),
+                              ctypes.POINTER(_SZ)]),
+    ("mmn_batch_upload", _I, [_P, _P, _SZ, _P]),
+    ("mmn_batch_run", _I, [_P, _P, _P]),
+    ("mmn_batch_info", _I, [_P, _I32P, _I32P, _I32P, _I32P]),
+    ("mmn_batch_destroy", None, [_P]),
     ("mmn_read_status", _I, [_P, _I32P, _P]),
 ]
 

@@ -82,3 +82,26 @@ def tune(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slo
     _cache[key] = res
     ops.set_variant(mode, best_idx if apply else 0)
     return res
+
+
+def tune_batched(objects, options=(4, 8, 16), repeats=1):
+    """Times the batched persistent launch for each work granularity (items per resident
+    CTA) and returns {"best": items_per_slot, "times_ms": {...}}."""
+    times = {}
+    for ips in options:
+        plan = ops.BatchPlan(objects, items_per_slot=ips)
+        plan.run()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(repeats):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plan.run()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        times[ips] = best
+        del plan
+    best_ips = min(times, key=times.get)
+    return {"best": best_ips, "times_ms": {str(k): v for k, v in times.items()}}

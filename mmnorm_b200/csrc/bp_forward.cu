@@ -51,10 +51,15 @@ constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im
 constexpr int kAnchorPoly = 0;
 constexpr int kAnchorFixed = 1;
 
-template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
-__global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
+// One work item: voxel tile `tile` of p against antenna split `split`.  The two stage
+// buffers' mbarriers are initialised by the caller; `gchunk` counts the chunks this CTA
+// has consumed so far (stage = gchunk & 1, phase parity = (gchunk >> 1) & 1), so a
+// persistent CTA can run item after item on the same barriers.  Returns false if a
+// bounded wait gave up (the status word is set).
+template <int T, int NT, int FORM, int ANCHOR>
+__device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split,
+                                         unsigned char *smem, uint32_t &gchunk) {
     static_assert(FORM != kFormMixedPair || T % 2 == 0, "pair form needs an even T");
-    extern __shared__ __align__(128) unsigned char smem[];
     Stage st;
     st.bars = reinterpret_cast<uint64_t *>(smem);
     st.base = smem + 128;
@@ -65,25 +70,19 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
     float *kappa_tab = reinterpret_cast<float *>(st.base + 2 * st.stage_bytes);  // PLAIN only
     const int fp = p.fp;
 
-    const int tile = blockIdx.x % p.num_tiles;
-    const int split = blockIdx.x / p.num_tiles;
     const int a_begin = split * p.ant_per_split;
     const int a_end = min(p.num_ant, a_begin + p.ant_per_split);
     const int n_chunks = a_end > a_begin ? (a_end - a_begin + st.nas - 1) / st.nas : 0;
+    const uint32_t g0 = gchunk;
 
-    if (threadIdx.x == 0) {
-        mbar_init(&st.bars[0], 1);
-        mbar_init(&st.bars[1], 1);
-        fence_mbar_init();
-    }
     if constexpr (FORM == kFormPlain) {
         for (int j = threadIdx.x; j < fp; j += NT)
             kappa_tab[j] = (float)fma((double)j, p.kd, p.k0);
+        __syncthreads();
     }
-    __syncthreads();
     if (threadIdx.x == 0) {
-        if (n_chunks > 0) st.issue(p, 0, a_begin, a_end);
-        if (n_chunks > 1) st.issue(p, 1, a_begin, a_end);
+        if (n_chunks > 0) st.issue(p, 0, (int)(g0 & 1), a_begin, a_end);
+        if (n_chunks > 1) st.issue(p, 1, (int)((g0 + 1) & 1), a_begin, a_end);
     }
 
     const int64_t rbase = (int64_t)tile * (NT * T) + threadIdx.x;
@@ -100,9 +99,10 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
     const int nblk = fp / kBlockF;
 
     for (int c = 0; c < n_chunks; ++c) {
-        const int s = c & 1;
-        bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
-        if (!__syncthreads_and(ok)) return;
+        const uint32_t gc = g0 + (uint32_t)c;
+        const int s = (int)(gc & 1);
+        bool ok = mbar_wait_bounded(&st.bars[s], (gc >> 1) & 1, p.status);
+        if (!__syncthreads_and(ok)) return false;
         const AntRec *ants = st.ants(s);
         const unsigned char *mstage = st.meas(s);
         const int na = min(st.nas, a_end - (a_begin + c * st.nas));
@@ -358,11 +358,53 @@ __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
+        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, s, a_begin, a_end);
     }
+    gchunk = g0 + (uint32_t)n_chunks;
 
 #pragma unroll
     for (int k = 0; k < T; ++k) store_voxel(p, split, rbase + (int64_t)k * NT, acc[k]);
+    return true;
+}
+
+__device__ __forceinline__ void init_stage_barriers(unsigned char *smem) {
+    if (threadIdx.x == 0) {
+        uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
+
+// One launch, grid = tiles x splits (one work item per CTA).
+template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
+__global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    init_stage_barriers(smem);
+    uint32_t gchunk = 0;
+    fwd_item<T, NT, FORM, ANCHOR>(p, blockIdx.x % p.num_tiles, blockIdx.x / p.num_tiles, smem,
+                                  gchunk);
+}
+
+// Persistent launch over a work list of (object, voxel tile, antenna split) items: every
+// CTA pops the next item from a global counter until the list is exhausted.  Items are
+// sorted by cost, largest first, so the tail is made of the smallest items.
+template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
+__global__ void __launch_bounds__(NT) bp_fwd_persistent(const BatchParams bp) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_item;
+    init_stage_barriers(smem);
+    uint32_t gchunk = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(bp.counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= bp.num_items) break;
+        const int4 w = bp.items[item];
+        if (!fwd_item<T, NT, FORM, ANCHOR>(bp.objs[w.x], w.y, w.z, smem, gchunk)) break;
+    }
 }
 
 __global__ void bp_reduce_partials(const FwdParams p) {
@@ -462,24 +504,28 @@ template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
 static const void *fwd_ptr() {
     return reinterpret_cast<const void *>(&bp_fwd_kernel<T, NT, FORM, ANCHOR>);
 }
+template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
+static const void *pers_ptr() {
+    return reinterpret_cast<const void *>(&bp_fwd_persistent<T, NT, FORM, ANCHOR>);
+}
 
 const FwdVariant *fwd_variants(int *count) {
     // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
-        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256", 1},
-        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t2_n256", 2},
-        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t1_n256", 2},
-        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t4_n128", 1},
-        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair>(), "mixed_antpair_t2_n256", 2},
-        {2, 128, false, 8, fwd_ptr<2, 128, kFormMixedAntPair>(), "mixed_antpair_t2_n128", 2},
-        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedAntPair>(), "mixed_antpair_t4_n128", 2},
-        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair>(), "mixed_antpair_t1_n256", 2},
-        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair>(), "mixed_ffma2_t4_n128", 1},
-        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair>(), "mixed_ffma2_t2_n256", 1},
-        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedScalar>(), "mixed_ffma_t4_n128", 0},
-        {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256", 0},
-        {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128", 0},
-        {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128", 0},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed>()},
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t2_n256", 2, pers_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>()},
+        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t1_n256", 2, pers_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>()},
+        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t4_n128", 1, pers_ptr<4, 128, kFormMixedPair, kAnchorFixed>()},
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair>(), "mixed_antpair_t2_n256", 2, pers_ptr<2, 256, kFormMixedAntPair>()},
+        {2, 128, false, 8, fwd_ptr<2, 128, kFormMixedAntPair>(), "mixed_antpair_t2_n128", 2, pers_ptr<2, 128, kFormMixedAntPair>()},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedAntPair>(), "mixed_antpair_t4_n128", 2, pers_ptr<4, 128, kFormMixedAntPair>()},
+        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair>(), "mixed_antpair_t1_n256", 2, pers_ptr<1, 256, kFormMixedAntPair>()},
+        {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair>(), "mixed_ffma2_t4_n128", 1, pers_ptr<4, 128, kFormMixedPair>()},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair>(), "mixed_ffma2_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair>()},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedScalar>(), "mixed_ffma_t4_n128", 0, pers_ptr<4, 128, kFormMixedScalar>()},
+        {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256", 0, nullptr},
+        {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128", 0, nullptr},
+        {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128", 0, nullptr},
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
     return v;

@@ -41,6 +41,16 @@ struct FwdVariant {
     const void *fn;
     const char *name;
     int layout; // staged sample layout (stage_meas): 0 (re,im), 1 (re,re,im,im), 2 antenna pairs
+    const void *persistent_fn;  // bp_fwd_persistent instantiation of the same form, or null
+};
+
+// Batched (persistent) forward: per-object FwdParams and a cost-sorted work list.
+struct BatchParams {
+    const FwdParams *objs;  // [num_objects]
+    const int4 *items;      // [num_items] (object, tile, split, -)
+    int32_t num_items;
+    int32_t pad0;
+    int *counter;           // work-list cursor, zeroed before each launch
 };
 
 const FwdVariant *fwd_variants(int *count);

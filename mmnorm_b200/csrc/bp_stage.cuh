@@ -15,8 +15,8 @@ struct Stage {
     int esz;  // bytes per sample in shared memory (8: (re, im); 16: (re, re, im, im))
     int fp;
 
-    __device__ void issue(const FwdParams &p, int c, int a_begin, int a_end) const {
-        const int s = c & 1;
+    // Fill stage buffer `s` with chunk `c` (antennas a_begin + c*nas ...) of a work item.
+    __device__ void issue(const FwdParams &p, int c, int s, int a_begin, int a_end) const {
         const int a0 = a_begin + c * nas;
         const int na = min(nas, a_end - a0);
         unsigned char *st = base + s * stage_bytes;
@@ -27,6 +27,9 @@ struct Stage {
         bulk_g2s(st + (size_t)nas * sizeof(AntRec),
                  static_cast<const unsigned char *>(p.meas) + (size_t)a0 * fp * esz,
                  meas_bytes, &bars[s]);
+    }
+    __device__ void issue(const FwdParams &p, int c, int a_begin, int a_end) const {
+        issue(p, c, c & 1, a_begin, a_end);
     }
     __device__ const AntRec *ants(int s) const {
         return reinterpret_cast<const AntRec *>(base + s * stage_bytes);

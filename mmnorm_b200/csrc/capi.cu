@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "bp_kernels.cuh"
 
@@ -772,3 +773,258 @@ extern "C" int mmn_backproject_noalloc(const mmn_problem *p, int32_t mode, float
                        reinterpret_cast<float2 *>(vote), nullptr, nullptr,
                        static_cast<unsigned char *>(scratch), stream);
 }
+
+// ---------------------------------------------------------------------------------
+// Batched persistent launch: many objects (uneven grids, apertures and sample counts)
+// in one launch over a cost-sorted (object, voxel tile, antenna split) work list.
+// ---------------------------------------------------------------------------------
+struct mmn_batch {
+    int n = 0;
+    int mode = 0;
+    const FwdVariant *var = nullptr;
+    size_t smem = 0;
+    int ctas = 0;
+    struct Obj {
+        int fp = 0, a_pad = 0, nas = 0, tiles = 0, splits = 1, aps = 0;
+        int64_t nvox = 0;
+        size_t off_ant = 0, off_meas = 0, off_partial = 0;
+    };
+    std::vector<mmn_problem> probs;
+    std::vector<Obj> obj;
+    std::vector<FwdParams> params;  // filled at upload (device pointers into the workspace)
+    std::vector<int4> items;
+    std::vector<float *> images, votes;
+    size_t off_flags = 0, off_counter = 0, off_params = 0, off_items = 0, total = 0;
+    void *uploaded_ws = nullptr;
+};
+
+extern "C" int mmn_batch_create(const mmn_problem *problems, int32_t num_objects, int32_t mode,
+                                float *const *images, float *const *votes,
+                                int32_t items_per_slot, mmn_batch **batch,
+                                size_t *workspace_bytes) {
+    if (!problems || !images || !batch || !workspace_bytes) return MMN_ERR_NULL_POINTER;
+    if (num_objects < 1 || mode != MMN_MODE_MIXED) return MMN_ERR_INVALID_ARGUMENT;
+    for (int o = 0; o < num_objects; ++o) {
+        const int rc = check_problem(&problems[o], mode);
+        if (rc != MMN_OK) return rc;
+        if (!images[o]) return MMN_ERR_NULL_POINTER;
+    }
+    if (items_per_slot <= 0) items_per_slot = 8;
+    int nvar = 0;
+    const FwdVariant *vars = fwd_variants(&nvar);
+    int vi = variant_index_for(mode);
+    if (vi < 0 || vi >= nvar || vars[vi].plain || !vars[vi].persistent_fn) {
+        vi = 0;
+        while (vi < nvar && (vars[vi].plain || !vars[vi].persistent_fn)) ++vi;
+        if (vi >= nvar) return MMN_ERR_UNSUPPORTED;
+    }
+    mmn_batch *b = new mmn_batch();
+    b->n = num_objects;
+    b->mode = mode;
+    b->var = &vars[vi];
+    b->probs.assign(problems, problems + num_objects);
+    b->images.assign(images, images + num_objects);
+    b->votes.assign(num_objects, nullptr);
+    if (votes)
+        for (int o = 0; o < num_objects; ++o) b->votes[o] = votes[o];
+    b->obj.resize(num_objects);
+    const bool pairs = b->var->layout == 2;
+    size_t max_stage = 0;
+    for (int o = 0; o < num_objects; ++o) {
+        auto &ob = b->obj[o];
+        const mmn_problem &p = problems[o];
+        ob.fp = (p.num_samples + kBlockF - 1) / kBlockF * kBlockF;
+        if (ob.fp > kMaxFp) {
+            delete b;
+            return MMN_ERR_TOO_LARGE;
+        }
+        ob.a_pad = pairs ? p.num_antennas + (p.num_antennas & 1) : p.num_antennas;
+        const int rec = (int)sizeof(AntRec) + ob.fp * b->var->esz;
+        ob.nas = std::max(1, std::min(16, kMaxStageBytes / rec));
+        if (pairs) ob.nas = std::max(2, ob.nas & ~1);
+        max_stage = std::max(max_stage, (size_t)ob.nas * rec);
+        ob.nvox = (int64_t)p.num_x * p.num_y * p.num_z;
+    }
+    b->smem = 128 + 2 * max_stage;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (b->smem > 48 * 1024)
+        cudaFuncSetAttribute(b->var->persistent_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)b->smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->var->persistent_fn, b->var->nt,
+                                                      b->smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    b->ctas = sms * per_sm;
+    // item granularity: about items_per_slot items per resident CTA
+    const int64_t tile_vox = (int64_t)b->var->nt * b->var->t;
+    double total_cost = 0;
+    for (int o = 0; o < num_objects; ++o)
+        total_cost += (double)b->obj[o].nvox * b->obj[o].a_pad * b->obj[o].fp;
+    const double target = std::max(1.0, total_cost / ((double)b->ctas * items_per_slot));
+    std::vector<std::pair<double, int4>> work;
+    for (int o = 0; o < num_objects; ++o) {
+        auto &ob = b->obj[o];
+        ob.tiles = (int)((ob.nvox + tile_vox - 1) / tile_vox);
+        if (ob.a_pad == 0) {
+            ob.splits = 0;
+            continue;
+        }
+        const double tile_cost = (double)tile_vox * ob.a_pad * ob.fp;
+        const int max_s = (ob.a_pad + ob.nas - 1) / ob.nas;
+        int s = (int)std::ceil(tile_cost / target);
+        s = std::max(1, std::min(s, std::min(max_s, 64)));
+        ob.aps = (ob.a_pad + s - 1) / s;
+        ob.aps = (ob.aps + ob.nas - 1) / ob.nas * ob.nas;
+        ob.splits = (ob.a_pad + ob.aps - 1) / ob.aps;
+        for (int t = 0; t < ob.tiles; ++t) {
+            const int64_t v = std::min<int64_t>(tile_vox, ob.nvox - (int64_t)t * tile_vox);
+            for (int sp = 0; sp < ob.splits; ++sp) {
+                const int na = std::min(ob.aps, ob.a_pad - sp * ob.aps);
+                work.push_back({(double)v * na * ob.fp, make_int4(o, t, sp, 0)});
+            }
+        }
+    }
+    std::stable_sort(work.begin(), work.end(),
+                     [](const std::pair<double, int4> &x, const std::pair<double, int4> &y) {
+                         return x.first > y.first;
+                     });
+    b->items.reserve(work.size());
+    for (auto &w : work) b->items.push_back(w.second);
+    // workspace layout
+    size_t off = kStatusBytes;
+    b->off_flags = off;
+    off = align_up(off + (size_t)num_objects * sizeof(int32_t));
+    b->off_counter = off;
+    off = align_up(off + sizeof(int));
+    b->off_params = off;
+    off = align_up(off + (size_t)num_objects * sizeof(FwdParams));
+    b->off_items = off;
+    off = align_up(off + b->items.size() * sizeof(int4) + 16);
+    for (int o = 0; o < num_objects; ++o) {
+        auto &ob = b->obj[o];
+        const int rows = b->var->layout == 2 ? ob.a_pad / 2 : ob.a_pad;
+        const size_t row_bytes = (size_t)ob.fp * (b->var->layout == 2 ? 16 : b->var->esz);
+        ob.off_ant = off;
+        off = align_up(off + (size_t)ob.a_pad * sizeof(AntRec));
+        ob.off_meas = off;
+        off = align_up(off + (size_t)rows * row_bytes);
+        ob.off_partial = off;
+        if (ob.splits > 1) off = align_up(off + (size_t)ob.splits * ob.nvox * 8 * sizeof(float));
+    }
+    b->total = off;
+    *batch = b;
+    *workspace_bytes = b->total;
+    return MMN_OK;
+}
+
+extern "C" int mmn_batch_upload(mmn_batch *b, void *workspace, size_t workspace_bytes,
+                                cudaStream_t stream) {
+    if (!b || !workspace) return MMN_ERR_NULL_POINTER;
+    if ((reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)) || workspace_bytes < b->total)
+        return MMN_ERR_WORKSPACE;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    b->params.assign(b->n, FwdParams());
+    for (int o = 0; o < b->n; ++o) {
+        const mmn_problem &p = b->probs[o];
+        const auto &ob = b->obj[o];
+        FwdParams &f = b->params[o];
+        std::memset(&f, 0, sizeof(f));
+        f.x_locs = p.x_locs;
+        f.y_locs = p.y_locs;
+        f.z_locs = p.z_locs;
+        f.nx = p.num_x;
+        f.ny = p.num_y;
+        f.nz = p.num_z;
+        f.nvox = ob.nvox;
+        f.vox_start = 0;
+        f.vox_count = ob.nvox;
+        f.ant = reinterpret_cast<const AntRec *>(ws + ob.off_ant);
+        f.meas = ws + ob.off_meas;
+        f.num_ant = ob.a_pad;
+        f.fp = ob.fp;
+        f.ant_per_stage = ob.nas;
+        f.mono_flag = reinterpret_cast<const int32_t *>(ws + b->off_flags) + o;
+        f.k0 = 2.0 * kPi / p.wavelength;
+        f.kd = 2.0 * kPi * p.slope / kC;
+        f.t0 = 1.0 / p.wavelength;
+        f.tblk = (double)kBlockF * p.slope / kC;
+        f.ti = p.is_ti_radar ? 0.15 : 0.0;
+        f.num_tiles = ob.tiles;
+        f.num_splits = std::max(1, ob.splits);
+        f.ant_per_split = ob.aps;
+        f.image = reinterpret_cast<float2 *>(b->images[o]);
+        f.vote = reinterpret_cast<float2 *>(b->votes[o]);
+        f.partial = reinterpret_cast<float4 *>(ws + ob.off_partial);
+        f.status = reinterpret_cast<int32_t *>(ws);
+    }
+    if (cudaMemcpyAsync(ws + b->off_params, b->params.data(), b->n * sizeof(FwdParams),
+                        cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    if (!b->items.empty() &&
+        cudaMemcpyAsync(ws + b->off_items, b->items.data(), b->items.size() * sizeof(int4),
+                        cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return MMN_ERR_CUDA;
+    b->uploaded_ws = workspace;
+    return MMN_OK;
+}
+
+extern "C" int mmn_batch_run(mmn_batch *b, void *workspace, cudaStream_t stream) {
+    if (!b || !workspace) return MMN_ERR_NULL_POINTER;
+    if (workspace != b->uploaded_ws) return MMN_ERR_WORKSPACE;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (cudaMemsetAsync(ws, 0, 16, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    if (cudaMemsetAsync(ws + b->off_counter, 0, sizeof(int), stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    for (int o = 0; o < b->n; ++o) {
+        const mmn_problem &p = b->probs[o];
+        const auto &ob = b->obj[o];
+        const int64_t V = ob.nvox;
+        if (p.num_antennas == 0) {
+            if (cudaMemsetAsync(b->images[o], 0, V * 8, stream) != cudaSuccess) return MMN_ERR_CUDA;
+            if (b->votes[o] && cudaMemsetAsync(b->votes[o], 0, 3 * V * 8, stream) != cudaSuccess)
+                return MMN_ERR_CUDA;
+            continue;
+        }
+        if (launch_prep_antennas(p.antenna_locs, p.rx_offsets, p.num_rx, p.pos_offsets,
+                                 p.num_antennas, ob.a_pad,
+                                 reinterpret_cast<AntRec *>(ws + ob.off_ant),
+                                 reinterpret_cast<int32_t *>(ws + b->off_flags) + o,
+                                 stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+        if (launch_stage_meas(p.meas, nullptr, p.num_antennas, p.num_samples, ob.fp,
+                              b->var->layout, ws + ob.off_meas, stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+    }
+    if (!b->items.empty()) {
+        BatchParams bp;
+        bp.objs = reinterpret_cast<const FwdParams *>(ws + b->off_params);
+        bp.items = reinterpret_cast<const int4 *>(ws + b->off_items);
+        bp.num_items = (int32_t)b->items.size();
+        bp.pad0 = 0;
+        bp.counter = reinterpret_cast<int *>(ws + b->off_counter);
+        void *args[] = {&bp};
+        const int grid = std::min<int>(b->ctas, (int)b->items.size());
+        if (cudaLaunchKernel(b->var->persistent_fn, dim3(grid), dim3(b->var->nt), args, b->smem,
+                             stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+    }
+    for (int o = 0; o < b->n; ++o)
+        if (b->obj[o].splits > 1 && launch_reduce(b->params[o], stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+    return MMN_OK;
+}
+
+extern "C" int mmn_batch_info(const mmn_batch *b, int32_t *num_items, int32_t *ctas,
+                              int32_t *threads, int32_t *voxels_per_thread) {
+    if (!b) return MMN_ERR_NULL_POINTER;
+    if (num_items) *num_items = (int32_t)b->items.size();
+    if (ctas) *ctas = b->ctas;
+    if (threads) *threads = b->var->nt;
+    if (voxels_per_thread) *voxels_per_thread = b->var->t;
+    return MMN_OK;
+}
+
+extern "C" void mmn_batch_destroy(mmn_batch *b) { delete b; }

@@ -246,3 +246,91 @@ def normals_differentiable(image, vote, eps=1e-30):
     mag = image.abs().clamp_min(eps)
     raw = (image.conj().unsqueeze(0) * vote).real / mag.unsqueeze(0)
     return raw / raw.norm(dim=0, keepdim=True).clamp_min(eps)
+
+
+class BatchPlan:
+    """Many objects in one persistent launch (mmn_batch_* in the C ABI).
+
+    ``objects``: sequence of dicts with CUDA tensors ``x_locs, y_locs, z_locs,
+    antenna_locs, rx_offsets, meas`` and scalars ``wavelength, slope`` (optional
+    ``is_ti_radar``, ``pos_offsets``).  ``run()`` computes every object's image and vote
+    into ``self.images[o]`` (complex64 [NX,NY,NZ]) and ``self.votes[o]``
+    (complex64 [3,NX,NY,NZ]); ``capture()`` records ``run()`` into a CUDA graph that
+    ``replay()`` re-launches.  The input tensors must stay alive and unmoved."""
+
+    def __init__(self, objects, items_per_slot=8, want_vote=True):
+        lib = _lib.load()
+        self.objects = list(objects)
+        n = len(self.objects)
+        dev = self.objects[0]["meas"].device
+        self.device = dev
+        probs = (_lib.MmnProblem * n)()
+        self.images, self.votes, self._shapes = [], [], []
+        for o, ob in enumerate(self.objects):
+            probs[o] = make_problem(ob["x_locs"], ob["y_locs"], ob["z_locs"], ob["antenna_locs"],
+                                    ob["rx_offsets"], ob["meas"], ob["wavelength"], ob["slope"],
+                                    0.0, ob.get("is_ti_radar", False), ob.get("pos_offsets"))
+            shape = (probs[o].num_x, probs[o].num_y, probs[o].num_z)
+            V = shape[0] * shape[1] * shape[2]
+            self._shapes.append(shape)
+            self.images.append(torch.empty(V, dtype=torch.complex64, device=dev))
+            self.votes.append(torch.empty((3, V), dtype=torch.complex64, device=dev)
+                              if want_vote else None)
+        img_ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() for t in self.images])
+        vote_ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() if t is not None else 0
+                                            for t in self.votes])
+        handle = ctypes.c_void_p()
+        nbytes = ctypes.c_size_t()
+        rc = lib.mmn_batch_create(probs, n, _lib.MODE_MIXED, ctypes.cast(img_ptrs, ctypes.c_void_p),
+                                  ctypes.cast(vote_ptrs, ctypes.c_void_p), int(items_per_slot),
+                                  ctypes.byref(handle), ctypes.byref(nbytes))
+        _lib.check(rc, "mmn_batch_create")
+        self._probs = probs
+        self._handle = handle
+        self.workspace = torch.empty(max(256, nbytes.value), dtype=torch.uint8, device=dev)
+        rc = lib.mmn_batch_upload(handle, _vp(self.workspace), self.workspace.numel(),
+                                  _stream(dev))
+        _lib.check(rc, "mmn_batch_upload")
+        self.graph = None
+
+    def info(self):
+        vals = [ctypes.c_int32() for _ in range(4)]
+        _lib.check(_lib.load().mmn_batch_info(self._handle, *[ctypes.byref(v) for v in vals]),
+                   "mmn_batch_info")
+        return dict(zip(("items", "ctas", "threads", "voxels_per_thread"), [v.value for v in vals]))
+
+    def run(self):
+        rc = _lib.load().mmn_batch_run(self._handle, _vp(self.workspace), _stream(self.device))
+        _lib.check(rc, "mmn_batch_run")
+
+    def capture(self):
+        """Record run() into a CUDA graph (warm-up run on a side stream first)."""
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.run()
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.run()
+        return self.graph
+
+    def replay(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def results(self):
+        out = []
+        for img, vote, shape in zip(self.images, self.votes, self._shapes):
+            out.append((img.view(*shape), vote.view(3, *shape) if vote is not None else None))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().mmn_batch_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
