@@ -56,7 +56,7 @@ constexpr int kAnchorFixed = 1;
 // has consumed so far (stage = gchunk & 1, phase parity = (gchunk >> 1) & 1), so a
 // persistent CTA can run item after item on the same barriers.  Returns false if a
 // bounded wait gave up (the status word is set).
-template <int T, int NT, int FORM, int ANCHOR>
+template <int T, int NT, int FORM, int ANCHOR, bool PERSISTENT>
 __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split,
                                          unsigned char *smem, uint32_t &gchunk) {
     static_assert(FORM != kFormMixedPair || T % 2 == 0, "pair form needs an even T");
@@ -73,13 +73,18 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
     const int a_begin = split * p.ant_per_split;
     const int a_end = min(p.num_ant, a_begin + p.ant_per_split);
     const int n_chunks = a_end > a_begin ? (a_end - a_begin + st.nas - 1) / st.nas : 0;
-    const uint32_t g0 = gchunk;
+    const uint32_t g0 = PERSISTENT ? gchunk : 0u;
 
+    if (!PERSISTENT && threadIdx.x == 0) {
+        mbar_init(&st.bars[0], 1);
+        mbar_init(&st.bars[1], 1);
+        fence_mbar_init();
+    }
     if constexpr (FORM == kFormPlain) {
         for (int j = threadIdx.x; j < fp; j += NT)
             kappa_tab[j] = (float)fma((double)j, p.kd, p.k0);
-        __syncthreads();
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
         if (n_chunks > 0) st.issue(p, 0, (int)(g0 & 1), a_begin, a_end);
         if (n_chunks > 1) st.issue(p, 1, (int)((g0 + 1) & 1), a_begin, a_end);
@@ -358,9 +363,9 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, s, a_begin, a_end);
+        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, (int)((g0 + (uint32_t)c) & 1), a_begin, a_end);
     }
-    gchunk = g0 + (uint32_t)n_chunks;
+    if (PERSISTENT) gchunk = g0 + (uint32_t)n_chunks;
 
 #pragma unroll
     for (int k = 0; k < T; ++k) store_voxel(p, split, rbase + (int64_t)k * NT, acc[k]);
@@ -381,10 +386,9 @@ __device__ __forceinline__ void init_stage_barriers(unsigned char *smem) {
 template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
 __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
-    init_stage_barriers(smem);
     uint32_t gchunk = 0;
-    fwd_item<T, NT, FORM, ANCHOR>(p, blockIdx.x % p.num_tiles, blockIdx.x / p.num_tiles, smem,
-                                  gchunk);
+    fwd_item<T, NT, FORM, ANCHOR, false>(p, blockIdx.x % p.num_tiles, blockIdx.x / p.num_tiles,
+                                         smem, gchunk);
 }
 
 // Persistent launch over a work list of (object, voxel tile, antenna split) items: every
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(NT) bp_fwd_persistent(const BatchParams bp) {
         __syncthreads();
         if (item >= bp.num_items) break;
         const int4 w = bp.items[item];
-        if (!fwd_item<T, NT, FORM, ANCHOR>(bp.objs[w.x], w.y, w.z, smem, gchunk)) break;
+        if (!fwd_item<T, NT, FORM, ANCHOR, true>(bp.objs[w.x], w.y, w.z, smem, gchunk)) break;
     }
 }
 
