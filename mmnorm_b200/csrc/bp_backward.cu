@@ -281,6 +281,236 @@ __global__ void __launch_bounds__(kMeasThreads) bp_bwd_meas_kernel(const BwdPara
     }
 }
 
+// ------------------------------------------------- measurement pass, warp per antenna
+// A CTA of NW warps covers NW consecutive antennas (one per warp); all warps stream the
+// same voxel records through shared memory.  Lane l takes voxel (chunk + 32i + l).  For
+// each 32-sample block the lane needs G*conj(p_t) for t = 0..31; it keeps the value of
+// sample t = i XOR l in register slot i.  Then a recursive-halving transpose-reduce over
+// the warp is select-free -- at every level each lane keeps slots [0, half) and sends
+// slots [half, 2*half) -- and slot 0 of lane l ends with the warp's sum for sample l.
+// Slot 0 is G * exp(+j d kappa_{32b + l}) (fixed-point phase, exact wrap); slot i is slot
+// (i - 2^k) times conj(z)^(+-2^k), 2^k the top bit of i, so every value is at most five
+// FP32 complex multiplies from its anchor.  Per (antenna, sample) the sum runs in a fixed
+// order: deterministic, no partial buffers.
+constexpr int kMeas2Warps = 8;
+constexpr int kMeas2Chunk = 512;  // voxel records per shared-memory chunk (24 KB)
+
+__device__ __forceinline__ void warp_transpose_reduce32(float (&v)[kBlockF]) {
+#pragma unroll
+    for (int level = 0; level < 5; ++level) {
+        const int half = 16 >> level;
+#pragma unroll
+        for (int i = 0; i < half; ++i) v[i] += __shfl_xor_sync(0xffffffffu, v[i + half], half);
+    }
+}
+
+template <int MAXB>
+__global__ void __launch_bounds__(kMeas2Warps * 32) bp_bwd_meas2_kernel(const BwdParams bp) {
+    const FwdParams &p = bp.f;
+    __shared__ float4 vrec[kMeas2Chunk * 3];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int a = blockIdx.x * kMeas2Warps + warp;
+    const bool active = a < bp.num_ant_real;
+    const AntRec ar = p.ant[active ? a : 0];
+    const bool mono = *p.mono_flag != 0;
+    const int nblk = p.fp / kBlockF;
+    const double t1 = p.tblk / kBlockF;  // turns per metre per sample step
+    float accr[MAXB], acci[MAXB];
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) accr[b] = acci[b] = 0.f;
+
+    for (int64_t v0 = 0; v0 < p.nvox; v0 += kMeas2Chunk) {
+        const int nv = (int)min((int64_t)kMeas2Chunk, p.nvox - v0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nv * 3; q += kMeas2Warps * 32) vrec[q] = bp.vox_rec[v0 * 3 + q];
+        __syncthreads();
+        if (!active) continue;
+        for (int base = 0; base < nv; base += 32) {
+            const int j = base + lane;
+            const bool vok = j < nv;
+            const float4 r0 = vrec[3 * (vok ? j : 0)];
+            const float4 r1 = vrec[3 * (vok ? j : 0) + 1];
+            const float4 r2 = vrec[3 * (vok ? j : 0) + 2];
+            const double d = range_fp64((double)r0.x, (double)r0.y, (double)r0.z, ar, mono, p.ti);
+            // conj(z)^(2^k), and its conjugate where lane bit k is set
+            float wr[5], wi[5];
+            {
+                const float2 z = cis_fp64_phase(d * p.kd);  // conj of the forward step
+                wr[0] = z.x;
+                wi[0] = z.y;
+#pragma unroll
+                for (int k = 1; k < 5; ++k) {
+                    wr[k] = wr[k - 1] * wr[k - 1] - wi[k - 1] * wi[k - 1];
+                    wi[k] = 2.f * wr[k - 1] * wi[k - 1];
+                }
+#pragma unroll
+                for (int k = 0; k < 5; ++k)
+                    if (lane & (1 << k)) wi[k] = -wi[k];
+            }
+            const float ux = ar.virt[0] - r0.x, uy = ar.virt[1] - r0.y, uz = ar.virt[2] - r0.z;
+            float Gr = fmaf(r2.z, uz, fmaf(r2.x, uy, fmaf(r1.z, ux, r1.x)));
+            float Gi = fmaf(r2.w, uz, fmaf(r2.y, uy, fmaf(r1.w, ux, r1.y)));
+            if (!vok) Gr = Gi = 0.f;
+            // phase of sample (32b + lane): turns d*(1/lambda + (32b + lane)*slope/c)
+            unsigned long long ph = turns_to_fixed(d * p.t0) +
+                                    (unsigned long long)lane * turns_to_fixed(d * t1);
+            const unsigned long long stp = turns_to_fixed(d * p.tblk);
+#pragma unroll 1
+            for (int b = 0; b < nblk; ++b) {
+                float ac, as;
+                fixed_cis(ph, ac, as);
+                ph += stp;
+                float qr[kBlockF], qi[kBlockF];
+                qr[0] = Gr * ac - Gi * as;
+                qi[0] = Gr * as + Gi * ac;
+#pragma unroll
+                for (int i = 1; i < kBlockF; ++i) {
+                    const int k = 31 - __clz(i);  // top bit of i (compile-time after unrolling)
+                    const int par = i - (1 << k);
+                    qr[i] = fmaf(qr[par], wr[k], -qi[par] * wi[k]);
+                    qi[i] = fmaf(qr[par], wi[k], qi[par] * wr[k]);
+                }
+                warp_transpose_reduce32(qr);
+                warp_transpose_reduce32(qi);
+#pragma unroll
+                for (int bb = 0; bb < MAXB; ++bb)
+                    if (bb == b) {
+                        accr[bb] += qr[0];
+                        acci[bb] += qi[0];
+                    }
+            }
+        }
+    }
+    if (!active) return;
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) {
+        const int j = b * kBlockF + lane;
+        if (b < nblk && j < bp.num_samples)
+            bp.grad_meas[(size_t)a * bp.num_samples + j] = make_float2(accr[b], acci[b]);
+    }
+}
+
+// Two voxels per lane (FFMA2 halves).  Slots are generated depth-first (parent =
+// slot - lowest set bit), so only the ancestor path is live; each pair is folded into one
+// scalar slot (the two voxels' sum) as soon as it exists, and one transpose-reduce then
+// serves 64 voxels.
+struct PairSteps {
+    float2 wr[5], wi[5], nwi[5];  // per-half step conj(z)^(2^k), conjugated where lane bit k is set
+};
+
+__host__ __device__ constexpr int dfs_child_bits(int i) { return i == 0 ? 5 : (i & 1 ? 0 : 1 + dfs_child_bits(i >> 1)); }
+
+template <int I>
+__device__ __forceinline__ void meas_dfs(float2 r, float2 m, const PairSteps &w,
+                                         float (&sr)[kBlockF], float (&si)[kBlockF]);
+
+// children of slot I are I + 2^k for k below I's lowest set bit, visited from the top bit down
+template <int I, int K>
+__device__ __forceinline__ void meas_dfs_children(float2 r, float2 m, const PairSteps &w,
+                                                  float (&sr)[kBlockF], float (&si)[kBlockF]) {
+    if constexpr (K > 0) {
+        constexpr int k = K - 1;
+        const float2 cr = __ffma2_rn(m, w.nwi[k], __fmul2_rn(r, w.wr[k]));
+        const float2 cm = __ffma2_rn(r, w.wi[k], __fmul2_rn(m, w.wr[k]));
+        meas_dfs<I + (1 << k)>(cr, cm, w, sr, si);
+        meas_dfs_children<I, K - 1>(r, m, w, sr, si);
+    }
+}
+
+template <int I>
+__device__ __forceinline__ void meas_dfs(float2 r, float2 m, const PairSteps &w,
+                                         float (&sr)[kBlockF], float (&si)[kBlockF]) {
+    sr[I] = r.x + r.y;
+    si[I] = m.x + m.y;
+    meas_dfs_children<I, dfs_child_bits(I)>(r, m, w, sr, si);
+}
+
+template <int MAXB>
+__global__ void __launch_bounds__(kMeas2Warps * 32) bp_bwd_meas3_kernel(const BwdParams bp) {
+    const FwdParams &p = bp.f;
+    __shared__ float4 vrec[kMeas2Chunk * 3];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int a = blockIdx.x * kMeas2Warps + warp;
+    const bool active = a < bp.num_ant_real;
+    const AntRec ar = p.ant[active ? a : 0];
+    const bool mono = *p.mono_flag != 0;
+    const int nblk = p.fp / kBlockF;
+    const double t1 = p.tblk / kBlockF;
+    float accr[MAXB], acci[MAXB];
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) accr[b] = acci[b] = 0.f;
+
+    for (int64_t v0 = 0; v0 < p.nvox; v0 += kMeas2Chunk) {
+        const int nv = (int)min((int64_t)kMeas2Chunk, p.nvox - v0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nv * 3; q += kMeas2Warps * 32) vrec[q] = bp.vox_rec[v0 * 3 + q];
+        __syncthreads();
+        if (!active) continue;
+        for (int base = 0; base < nv; base += 64) {
+            PairSteps w;
+            float2 gr, gi;
+            unsigned long long ph[2], stp[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = base + 32 * h + lane;
+                const bool vok = j < nv;
+                const float4 r0 = vrec[3 * (vok ? j : 0)];
+                const float4 r1 = vrec[3 * (vok ? j : 0) + 1];
+                const float4 r2 = vrec[3 * (vok ? j : 0) + 2];
+                const double d =
+                    range_fp64((double)r0.x, (double)r0.y, (double)r0.z, ar, mono, p.ti);
+                const float2 z = cis_fp64_phase(d * p.kd);  // conj of the forward step
+                float zr = z.x, zi = z.y;
+#pragma unroll
+                for (int k = 0; k < 5; ++k) {
+                    const float si = (lane & (1 << k)) ? -zi : zi;
+                    (h ? w.wr[k].y : w.wr[k].x) = zr;
+                    (h ? w.wi[k].y : w.wi[k].x) = si;
+                    (h ? w.nwi[k].y : w.nwi[k].x) = -si;
+                    const float nr = zr * zr - zi * zi;
+                    zi = 2.f * zr * zi;
+                    zr = nr;
+                }
+                const float ux = ar.virt[0] - r0.x, uy = ar.virt[1] - r0.y, uz = ar.virt[2] - r0.z;
+                float Gr = fmaf(r2.z, uz, fmaf(r2.x, uy, fmaf(r1.z, ux, r1.x)));
+                float Gi = fmaf(r2.w, uz, fmaf(r2.y, uy, fmaf(r1.w, ux, r1.y)));
+                if (!vok) Gr = Gi = 0.f;
+                (h ? gr.y : gr.x) = Gr;
+                (h ? gi.y : gi.x) = Gi;
+                ph[h] = turns_to_fixed(d * p.t0) + (unsigned long long)lane * turns_to_fixed(d * t1);
+                stp[h] = turns_to_fixed(d * p.tblk);
+            }
+#pragma unroll 1
+            for (int b = 0; b < nblk; ++b) {
+                float2 ac, as;
+                fixed_cis(ph[0], ac.x, as.x);
+                fixed_cis(ph[1], ac.y, as.y);
+                ph[0] += stp[0];
+                ph[1] += stp[1];
+                float sr[kBlockF], si[kBlockF];
+                // slot 0: G * anchor (both halves), then the depth-first slot tree
+                meas_dfs<0>(__ffma2_rn(gr, ac, __fmul2_rn(gi, make_float2(-as.x, -as.y))),
+                            __ffma2_rn(gr, as, __fmul2_rn(gi, ac)), w, sr, si);
+                warp_transpose_reduce32(sr);
+                warp_transpose_reduce32(si);
+#pragma unroll
+                for (int bb = 0; bb < MAXB; ++bb)
+                    if (bb == b) {
+                        accr[bb] += sr[0];
+                        acci[bb] += si[0];
+                    }
+            }
+        }
+    }
+    if (!active) return;
+#pragma unroll
+    for (int b = 0; b < MAXB; ++b) {
+        const int j = b * kBlockF + lane;
+        if (b < nblk && j < bp.num_samples)
+            bp.grad_meas[(size_t)a * bp.num_samples + j] = make_float2(accr[b], acci[b]);
+    }
+}
+
 // -------------------------------------------------------------------- launchers
 const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread) {
     if (variant == 1) {
@@ -326,8 +556,18 @@ cudaError_t launch_bwd_pos_reduce(const BwdParams &bp, cudaStream_t stream) {
 }
 
 cudaError_t launch_bwd_meas(const BwdParams &bp, cudaStream_t stream) {
-    const int blocks = (bp.num_items + kMeasThreads - 1) / kMeasThreads;
-    bp_bwd_meas_kernel<<<blocks, kMeasThreads, 0, stream>>>(bp);
+    const int nblk = bp.f.fp / kBlockF;
+    const int blocks2 = (bp.num_ant_real + kMeas2Warps - 1) / kMeas2Warps;
+    if (nblk <= 4) {
+        bp_bwd_meas3_kernel<4><<<blocks2, kMeas2Warps * 32, 0, stream>>>(bp);
+    } else if (nblk <= 8) {
+        bp_bwd_meas3_kernel<8><<<blocks2, kMeas2Warps * 32, 0, stream>>>(bp);
+    } else if (nblk <= 16) {
+        bp_bwd_meas2_kernel<16><<<blocks2, kMeas2Warps * 32, 0, stream>>>(bp);
+    } else {
+        const int blocks = (bp.num_items + kMeasThreads - 1) / kMeasThreads;
+        bp_bwd_meas_kernel<<<blocks, kMeasThreads, 0, stream>>>(bp);
+    }
     return cudaGetLastError();
 }
 
