@@ -221,7 +221,7 @@ def ours_arm(args):
     import torch
     import torch.distributed as dist
 
-    from mmnorm_b200 import _lib, autotune, ops
+    from mmnorm_b200 import _lib, autotune, ops, shard
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -237,10 +237,21 @@ def ours_arm(args):
 
     sc = load_scene(dev, args.aperture)
     A, F = sc.meas.shape
-    V = sc.num_voxels
-    updates = V * A * F
     t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
-    xs, ys, zs = t(sc.x_locs), t(sc.y_locs), t(sc.z_locs)
+    # N GPUs: the grid grows by one 128-plane slab per GPU along x (same pitch, centred
+    # on the scene) and every rank images its own slab (voxel-slab sharding, weak scaling)
+    nx_total = len(sc.x_locs) * world
+    if world > 1:
+        pitch = float(sc.x_locs[1] - sc.x_locs[0])
+        x_all = (float(np.mean(sc.x_locs)) +
+                 (np.arange(nx_total) - (nx_total - 1) / 2.0) * pitch).astype(np.float32)
+        x0, x1 = shard.split_bounds(nx_total, world, rank)
+        xs = t(x_all[x0:x1])
+    else:
+        xs = t(sc.x_locs)
+    ys, zs = t(sc.y_locs), t(sc.z_locs)
+    V = xs.numel() * ys.numel() * zs.numel()
+    updates = V * A * F
     ant, rxo = t(sc.antenna_locs), t(np.zeros((1, 3), np.float32))
     meas = t(sc.meas)
     if args.variant:
@@ -256,6 +267,8 @@ def ours_arm(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
+    max_abs = torch.empty(1, dtype=torch.float32, device=dev)
+
     def step(mode="mixed", ev=None):
         flush.fill_(1)
         if ev is not None:
@@ -264,7 +277,11 @@ def ours_arm(args):
                                     mode=mode, workspace=ws)
         if ev is not None:
             ev[1].record(stream)
-        normals, mask = ops.surface_normals(img, vote, 0.05)
+        # mask threshold: 5 % of max|I| over the whole grid (one float all-reduced)
+        ops.image_max_abs(img, out=max_abs)
+        if world > 1:
+            dist.all_reduce(max_abs, op=dist.ReduceOp.MAX)
+        normals, mask = ops.surface_normals_from_max(img, vote, max_abs, 0.05)
         return img, vote, normals, mask
 
     def barrier():
@@ -312,7 +329,8 @@ def ours_arm(args):
     value = world * updates * args.steps / (total_ms * 1e-3) / 1e9
     kern_ms = [a.elapsed_time(b) for a, b in kernel_events]
     kern_avg_s = statistics.mean(kern_ms) * 1e-3
-    launches_per_step = 4 + (1 if plan["splits"] > 1 else 0)
+    # prep_antennas, stage_meas, bp_fwd_kernel (+ bp_reduce_partials), max_abs, normals
+    launches_per_step = 5 + (1 if plan["splits"] > 1 else 0)
 
     out = {}
     if rank == 0 and world == 1 and args.plain_steps > 0:
@@ -398,6 +416,25 @@ def ours_arm(args):
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": "failed: %s" % str(e)[:200]}
 
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+
+    def lane_bounds(rate, updates_per_sm_clock):
+        """Fraction of the SM-count x clock x lanes bound (128 FP32 lanes per SM per clock
+        over 8 lane-ops per update; 16 SFU results per SM per clock over 2 per update) at
+        the sampled loaded clock and at the maximum clock."""
+        out = {}
+        for label, mhz in (("at_sampled_clock", clk.get("sm_mhz")),
+                           ("at_max_clock", clk.get("sm_max_mhz"))):
+            if mhz:
+                bound = sms * mhz * 1e6 * updates_per_sm_clock
+                out[label] = {"sm_mhz": mhz, "bound_G_updates_per_s": bound / 1e9,
+                              "frac": rate / bound}
+        return out
+
+    if "plain" in out:
+        out["plain"]["sfu_bound"] = lane_bounds(updates / (out["plain"]["kernel_ms"] * 1e-3),
+                                                16 / 2)
+
     if rank == 0:
         flops = 8.0 * updates          # one complex multiply-add (4 FFMA) per update
         achieved = flops / kern_avg_s / 1e12
@@ -412,8 +449,11 @@ def ours_arm(args):
             "data": "synthetic (seeded point-scatterer scene, exp(-j4pi f r/c)/r^2, 15 dB)",
             "config": {"workload": sc.name + " (128^3 voxels @2 mm, 128x128 antennas @2 mm, "
                        "256 freqs 77-81 GHz; image + vote + unit normals)",
-                       "voxels": V, "antennas": A, "freqs": F,
-                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "voxels": V * world, "voxels_per_gpu": V, "antennas": A, "freqs": F,
+                       "parallelism": ("voxel slabs: %d x-planes of a %d x %d x %d grid per "
+                                       "GPU, one all-reduce(MAX) of max|I| per step"
+                                       % (xs.numel(), nx_total, ys.numel(), zs.numel()))
+                       if world > 1 else "single GPU",
                        "l2": "flushed before every step (256 MB write)",
                        "plan": plan, "variant": variant["name"],
                        "autotune_ms": tuned["times_ms"]},
@@ -424,7 +464,8 @@ def ours_arm(args):
                          "flops_per_update": 8,
                          "peak_source": "FP32 FFMA probe (mmn_fp32_peak_probe) timed in this "
                                         "run; MEASURED_PEAKS.json has no FP32 figure",
-                         "kernel_ms": statistics.mean(kern_ms)},
+                         "kernel_ms": statistics.mean(kern_ms),
+                         "fp32_lane_bound": lane_bounds(updates / kern_avg_s, 128 / 8)},
             "clocks": clk,
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,

@@ -174,6 +174,22 @@ int mmn_normals(int64_t num_voxels, const float *image, const float *vote,
                 void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /*
+ * The two halves of mmn_normals, for a grid split into voxel slabs over several GPUs
+ * (the reference splits the voxel range the same way through start_ind,
+ * py_image_gpu.py:187,273): the mask threshold needs the maximum |I| over the WHOLE
+ * grid, so each slab takes its local maximum, the caller combines them (an all-reduce
+ * of one float with MAX), and each slab then finishes its normals against the global
+ * value.
+ * mmn_image_max_abs: *max_abs (device, one float) = max |image[v]| over the slab.
+ * mmn_normals_from_max: as mmn_normals, with max|I| read from *max_abs (device).
+ */
+int mmn_image_max_abs(int64_t num_voxels, const float *image, float *max_abs,
+                      cudaStream_t stream);
+int mmn_normals_from_max(int64_t num_voxels, const float *image, const float *vote,
+                         const float *max_abs, float filter_percent, float *normals,
+                         uint8_t *mask, float *raw, cudaStream_t stream);
+
+/*
  * Drop-in for the reference kernel launch `cuda_image`
  * (src/data_processing/cuda/imaging_gpu.cu:12-21, launched at py_image_gpu.py:189-199):
  * same arguments in the same order and meaning (SoA measurements, float scalars,

@@ -82,6 +82,8 @@ SIGNATURES = [
     ("mmn_backproject_backward", _I, [_PROB, _P, _P, _P, _P, _P, _SZ, _P]),
     ("mmn_normals_workspace_bytes", _SZ, [ctypes.c_int64]),
     ("mmn_normals", _I, [ctypes.c_int64, _P, _P, _F, _P, _P, _P, _P, _SZ, _P]),
+    ("mmn_image_max_abs", _I, [ctypes.c_int64, _P, _P, _P]),
+    ("mmn_normals_from_max", _I, [ctypes.c_int64, _P, _P, _P, _F, _P, _P, _P, _P]),
     ("mmn_cuda_image_workspace_bytes", _SZ, [_I, _I, _I]),
     ("mmn_cuda_image_workspace_bytes_for", _SZ, [_I, _I, _I, _I, _I, _I, _I, _I]),
     ("mmn_cuda_image", _I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _F, _F, _F, _I, _I, _I, _I,

@@ -60,9 +60,8 @@ __global__ void normals_kernel(const float2 *__restrict__ image, const float2 *_
     if (mask) mask[v] = in ? 1 : 0;
 }
 
-cudaError_t launch_normals(int64_t nvox, const float2 *image, const float2 *vote,
-                           float filter_percent, float *normals, uint8_t *mask, float *raw,
-                           unsigned int *max_bits, cudaStream_t stream) {
+cudaError_t launch_max_abs(int64_t nvox, const float2 *image, unsigned int *max_bits,
+                           cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(max_bits, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148;
@@ -73,12 +72,27 @@ cudaError_t launch_normals(int64_t nvox, const float2 *image, const float2 *vote
     if (blocks > 4 * sms) blocks = 4 * sms;
     if (blocks < 1) blocks = 1;
     max_abs_kernel<<<(unsigned)blocks, nt, 0, stream>>>(image, nvox, max_bits);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normals_from_max(int64_t nvox, const float2 *image, const float2 *vote,
+                                    float filter_percent, float *normals, uint8_t *mask,
+                                    float *raw, const unsigned int *max_bits,
+                                    cudaStream_t stream) {
+    const int nt = 256;
     const int64_t b2 = (nvox + nt - 1) / nt;
     normals_kernel<<<(unsigned)b2, nt, 0, stream>>>(image, vote, nvox, filter_percent, max_bits,
                                                     normals, mask, raw);
     return cudaGetLastError();
+}
+
+cudaError_t launch_normals(int64_t nvox, const float2 *image, const float2 *vote,
+                           float filter_percent, float *normals, uint8_t *mask, float *raw,
+                           unsigned int *max_bits, cudaStream_t stream) {
+    cudaError_t e = launch_max_abs(nvox, image, max_bits, stream);
+    if (e != cudaSuccess) return e;
+    return launch_normals_from_max(nvox, image, vote, filter_percent, normals, mask, raw,
+                                   max_bits, stream);
 }
 
 }  // namespace mmn

@@ -117,6 +117,12 @@ cudaError_t launch_interp_image(const InterpParams &p, cudaStream_t stream);
 cudaError_t launch_interp_normals(const InterpParams &p, cudaStream_t stream);
 
 // --------------------------------------------------------------------- epilogue
+cudaError_t launch_max_abs(int64_t nvox, const float2 *image, unsigned int *max_bits,
+                           cudaStream_t stream);
+cudaError_t launch_normals_from_max(int64_t nvox, const float2 *image, const float2 *vote,
+                                    float filter_percent, float *normals, uint8_t *mask,
+                                    float *raw, const unsigned int *max_bits,
+                                    cudaStream_t stream);
 cudaError_t launch_normals(int64_t nvox, const float2 *image, const float2 *vote,
                            float filter_percent, float *normals, uint8_t *mask, float *raw,
                            unsigned int *max_bits, cudaStream_t stream);

@@ -366,6 +366,33 @@ int mmn_normals(int64_t num_voxels, const float *image, const float *vote, float
     return e == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
 }
 
+int mmn_image_max_abs(int64_t num_voxels, const float *image, float *max_abs,
+                      cudaStream_t stream) {
+    if (num_voxels < 1) return MMN_ERR_INVALID_ARGUMENT;
+    if (!image || !max_abs) return MMN_ERR_NULL_POINTER;
+    if (reinterpret_cast<uintptr_t>(max_abs) & 3) return MMN_ERR_INVALID_ARGUMENT;
+    // |I| >= 0, so the float's bit pattern orders like the value: atomicMax on the bits
+    cudaError_t e = launch_max_abs(num_voxels, reinterpret_cast<const float2 *>(image),
+                                   reinterpret_cast<unsigned int *>(max_abs), stream);
+    return e == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+}
+
+int mmn_normals_from_max(int64_t num_voxels, const float *image, const float *vote,
+                         const float *max_abs, float filter_percent, float *normals,
+                         uint8_t *mask, float *raw, cudaStream_t stream) {
+    if (num_voxels < 1) return MMN_ERR_INVALID_ARGUMENT;
+    if (!image || !vote || !max_abs) return MMN_ERR_NULL_POINTER;
+    if (!normals && !mask && !raw) return MMN_ERR_NULL_POINTER;
+    if (reinterpret_cast<uintptr_t>(max_abs) & 3) return MMN_ERR_INVALID_ARGUMENT;
+    if (!(filter_percent >= 0.f) || !std::isfinite(filter_percent))
+        return MMN_ERR_INVALID_ARGUMENT;
+    cudaError_t e = launch_normals_from_max(
+        num_voxels, reinterpret_cast<const float2 *>(image),
+        reinterpret_cast<const float2 *>(vote), filter_percent, normals, mask, raw,
+        reinterpret_cast<const unsigned int *>(max_abs), stream);
+    return e == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+}
+
 size_t mmn_cuda_image_workspace_bytes(int num_antennas, int samples_per_meas,
                                       int use_interpolated_processing) {
     if (use_interpolated_processing) return kStatusBytes;

@@ -145,6 +145,42 @@ def surface_normals(image, vote, filter_percent=0.05, want_raw=False):
     return out
 
 
+def image_max_abs(image, out=None):
+    """max |image| as a float32 device tensor of one element (``out`` if given)."""
+    dev = image.device
+    img = _need(image.reshape(-1), "image", torch.complex64, dev)
+    if out is None:
+        out = torch.empty(1, dtype=torch.float32, device=dev)
+    _need(out, "out", torch.float32, dev, (1,))
+    _lib.check(_lib.load().mmn_image_max_abs(img.numel(), _vp(img), _vp(out), _stream(dev)),
+               "mmn_image_max_abs")
+    return out
+
+
+def surface_normals_from_max(image, vote, max_abs, filter_percent=0.05, want_raw=False):
+    """surface_normals with the mask threshold taken from ``max_abs`` (float32 device
+    tensor of one element, e.g. the all-reduced maximum over every slab of a grid)."""
+    dev = image.device
+    shape = tuple(image.shape)
+    V = image.numel()
+    img = image.reshape(V)
+    w = vote.reshape(3, V)
+    _need(img, "image", torch.complex64, dev)
+    _need(w, "vote", torch.complex64, dev)
+    _need(max_abs, "max_abs", torch.float32, dev, (1,))
+    normals = torch.empty((V, 3), dtype=torch.float32, device=dev)
+    mask = torch.empty(V, dtype=torch.uint8, device=dev)
+    raw = torch.empty((V, 3), dtype=torch.float32, device=dev) if want_raw else None
+    rc = _lib.load().mmn_normals_from_max(V, _vp(img), _vp(w), _vp(max_abs),
+                                          float(filter_percent), _vp(normals), _vp(mask),
+                                          _vp(raw), _stream(dev))
+    _lib.check(rc, "mmn_normals_from_max")
+    out = (normals.view(*shape, 3), mask.view(shape).bool())
+    if want_raw:
+        out = out + (raw.view(*shape, 3),)
+    return out
+
+
 def read_status(workspace):
     """Synchronise and return (and clear) the in-kernel status word of a workspace."""
     st = ctypes.c_int32(0)
