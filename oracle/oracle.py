@@ -234,7 +234,7 @@ def ref_prep(radar_data, rx_offsets, antenna_locs, use_4_rx):
 def ref_image_cuda(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offsets, slope,
                    wavelength, bandwidth, num_samples, use_4_rx=False, is_ti_radar=False,
                    use_interpolated_processing=False, return_phase_centers=True,
-                   dist_mode=0):
+                   dist_mode=0, max_num_ant=4096 * 32):
     """Restatement of py_image_gpu.image_cuda (py_image_gpu.py:308-366) over the FP64
     oracle kernels.  Returns the complex128 image [NX,NY,NZ] (and phase centres)."""
     vox = _grid_vox(x_locs, y_locs, z_locs)
@@ -263,7 +263,6 @@ def ref_image_cuda(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offsets,
         img = img / np.asarray(antenna_locs).shape[0]
         cl = centres(locs_rep)
     else:
-        max_num_ant = 4096 * 32
         num_rx = len(rx_offsets)
         groups = math.ceil(np.asarray(antenna_locs).shape[0] * num_rx / max_num_ant)
         img, cl = None, None
@@ -279,7 +278,8 @@ def ref_image_cuda(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offsets,
 def ref_normal_estimates_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs,
                               radar_data, rx_offset, slope, wavelength, bandwidth,
                               num_samples, use_4_rx=False, is_ti_radar=False,
-                              initial_filter_percent=0.05, dist_mode=0):
+                              initial_filter_percent=0.05, dist_mode=0,
+                              max_num_ant=4096 * 32):
     """Restatement of py_sn_est_gpu.normal_estimates_cuda (interpolated mode,
     py_sn_est_gpu.py:291-424): float64 [NX,NY,NZ,3], NaN outside the mask, not unit."""
     sum_image = np.asarray(sum_image)
@@ -290,7 +290,6 @@ def ref_normal_estimates_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs,
     vox = vox_all[flat]
     vals = sum_image.ravel()[flat].astype(np.complex64)
     rx_offset = np.asarray(rx_offset)
-    max_num_ant = 4096 * 32
     num_rx = len(rx_offset)
     groups = math.ceil(np.asarray(antenna_locs).shape[0] * num_rx / max_num_ant)
     total = None
