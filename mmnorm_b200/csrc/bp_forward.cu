@@ -527,6 +527,14 @@ const FwdVariant *fwd_variants(int *count) {
         {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair>(), "mixed_ffma2_t4_n128", 1, pers_ptr<4, 128, kFormMixedPair>()},
         {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair>(), "mixed_ffma2_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair>()},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedScalar>(), "mixed_ffma_t4_n128", 0, pers_ptr<4, 128, kFormMixedScalar>()},
+        // the default form with smaller stages: more CTAs per SM (occupancy is limited by
+        // two 48 KB stages otherwise), at the cost of more stage hand-overs
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256_s24", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), 24 * 1024},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256_s16", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), 16 * 1024},
+        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n128_s24", 1, pers_ptr<2, 128, kFormMixedPair, kAnchorFixed>(), 24 * 1024},
+        // two voxel pairs per thread: one shared load feeds 8 FFMA2 (the stages limit
+        // occupancy to two CTAs per SM either way, which leaves 128 registers a thread)
+        {4, 256, false, 16, fwd_ptr<4, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t4_n256", 1, pers_ptr<4, 256, kFormMixedPair, kAnchorFixed>()},
         {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256", 0, nullptr},
         {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128", 0, nullptr},
         {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128", 0, nullptr},

@@ -42,6 +42,7 @@ struct FwdVariant {
     const char *name;
     int layout; // staged sample layout (stage_meas): 0 (re,im), 1 (re,re,im,im), 2 antenna pairs
     const void *persistent_fn;  // bp_fwd_persistent instantiation of the same form, or null
+    int max_stage_bytes;        // cap on one shared-memory stage; 0: the library default
 };
 
 // Batched (persistent) forward: per-object FwdParams and a cost-sorted work list.

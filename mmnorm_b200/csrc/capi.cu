@@ -73,7 +73,8 @@ int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int 
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
     const int esz = pl->var->esz;
     const int rec = (int)sizeof(AntRec) + pl->fp * esz;
-    pl->ant_per_stage = std::max(1, std::min(16, kMaxStageBytes / rec));
+    const int cap = pl->var->max_stage_bytes > 0 ? pl->var->max_stage_bytes : kMaxStageBytes;
+    pl->ant_per_stage = std::max(1, std::min(16, cap / rec));
     if (pairs) pl->ant_per_stage = std::max(2, pl->ant_per_stage & ~1);
     pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec + (pl->var->plain ? pl->fp * 4 : 0);
     pl->vox_start = vox_start;
@@ -867,7 +868,8 @@ extern "C" int mmn_batch_create(const mmn_problem *problems, int32_t num_objects
         }
         ob.a_pad = pairs ? p.num_antennas + (p.num_antennas & 1) : p.num_antennas;
         const int rec = (int)sizeof(AntRec) + ob.fp * b->var->esz;
-        ob.nas = std::max(1, std::min(16, kMaxStageBytes / rec));
+        const int cap = b->var->max_stage_bytes > 0 ? b->var->max_stage_bytes : kMaxStageBytes;
+        ob.nas = std::max(1, std::min(16, cap / rec));
         if (pairs) ob.nas = std::max(2, ob.nas & ~1);
         max_stage = std::max(max_stage, (size_t)ob.nas * rec);
         ob.nvox = (int64_t)p.num_x * p.num_y * p.num_z;

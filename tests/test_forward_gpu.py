@@ -147,7 +147,7 @@ def test_deterministic_and_status_clean(cuda_dev):
     assert ops.read_status(ws) == 0
 
 
-@pytest.mark.parametrize("idx", list(range(12)))
+@pytest.mark.parametrize("idx", list(range(16)))
 def test_every_mixed_variant(cuda_dev, oracle, idx):
     from mmnorm_b200 import ops
     n = len(ops.variants("mixed"))
