@@ -425,12 +425,16 @@ __device__ __forceinline__ void meas_dfs(float2 r, float2 m, const PairSteps &w,
     meas_dfs_children<I, dfs_child_bits(I)>(r, m, w, sr, si);
 }
 
-template <int MAXB>
-__global__ void __launch_bounds__(kMeas2Warps * 32) bp_bwd_meas3_kernel(const BwdParams bp) {
+// Grid: (antennas / NW) x meas_splits; CTA (x, s) covers voxel range s, and with several
+// ranges writes its sums to the range's partial buffer (reduced in range order after).
+template <int MAXB, int NW>
+__global__ void __launch_bounds__(NW * 32) bp_bwd_meas3_kernel(const BwdParams bp) {
     const FwdParams &p = bp.f;
     __shared__ float4 vrec[kMeas2Chunk * 3];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int a = blockIdx.x * kMeas2Warps + warp;
+    const int a = blockIdx.x * NW + warp;
+    const int64_t v_begin = (int64_t)blockIdx.y * bp.vox_per_split;
+    const int64_t v_end = min(p.nvox, v_begin + bp.vox_per_split);
     const bool active = a < bp.num_ant_real;
     const AntRec ar = p.ant[active ? a : 0];
     const bool mono = *p.mono_flag != 0;
@@ -440,10 +444,10 @@ __global__ void __launch_bounds__(kMeas2Warps * 32) bp_bwd_meas3_kernel(const Bw
 #pragma unroll
     for (int b = 0; b < MAXB; ++b) accr[b] = acci[b] = 0.f;
 
-    for (int64_t v0 = 0; v0 < p.nvox; v0 += kMeas2Chunk) {
-        const int nv = (int)min((int64_t)kMeas2Chunk, p.nvox - v0);
+    for (int64_t v0 = v_begin; v0 < v_end; v0 += kMeas2Chunk) {
+        const int nv = (int)min((int64_t)kMeas2Chunk, v_end - v0);
         __syncthreads();
-        for (int q = threadIdx.x; q < nv * 3; q += kMeas2Warps * 32) vrec[q] = bp.vox_rec[v0 * 3 + q];
+        for (int q = threadIdx.x; q < nv * 3; q += NW * 32) vrec[q] = bp.vox_rec[v0 * 3 + q];
         __syncthreads();
         if (!active) continue;
         for (int base = 0; base < nv; base += 64) {
@@ -503,12 +507,28 @@ __global__ void __launch_bounds__(kMeas2Warps * 32) bp_bwd_meas3_kernel(const Bw
         }
     }
     if (!active) return;
+    float2 *dst = bp.meas_splits > 1
+                      ? bp.meas_partial + ((size_t)blockIdx.y * bp.num_ant_real + a) * bp.num_samples
+                      : bp.grad_meas + (size_t)a * bp.num_samples;
 #pragma unroll
     for (int b = 0; b < MAXB; ++b) {
         const int j = b * kBlockF + lane;
-        if (b < nblk && j < bp.num_samples)
-            bp.grad_meas[(size_t)a * bp.num_samples + j] = make_float2(accr[b], acci[b]);
+        if (b < nblk && j < bp.num_samples) dst[j] = make_float2(accr[b], acci[b]);
     }
+}
+
+// grad_meas = the voxel ranges' partial sums, added in range order (deterministic)
+__global__ void bwd_meas_reduce_kernel(const BwdParams bp) {
+    const int64_t n = (int64_t)bp.num_ant_real * bp.num_samples;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float2 s = bp.meas_partial[i];
+    for (int k = 1; k < bp.meas_splits; ++k) {
+        const float2 v = bp.meas_partial[(size_t)k * n + i];
+        s.x += v.x;
+        s.y += v.y;
+    }
+    bp.grad_meas[i] = s;
 }
 
 // -------------------------------------------------------------------- launchers
@@ -555,13 +575,50 @@ cudaError_t launch_bwd_pos_reduce(const BwdParams &bp, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+constexpr int kMeas3Warps = 4;  // 4 warps per CTA: three CTAs per SM at ~150 registers
+
+int bwd_meas_splits(int num_ant, int fp, int64_t nvox) {
+    const int nblk = fp / kBlockF;
+    if (nblk > 8 || num_ant < 1 || nvox < 1) return 1;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const void *fn = nblk <= 4 ? reinterpret_cast<const void *>(&bp_bwd_meas3_kernel<4, kMeas3Warps>)
+                               : reinterpret_cast<const void *>(&bp_bwd_meas3_kernel<8, kMeas3Warps>);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMeas3Warps * 32, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int64_t slots = (int64_t)sms * per_sm;
+    const int64_t bx = (num_ant + kMeas3Warps - 1) / kMeas3Warps;
+    const int64_t chunks = (nvox + kMeas2Chunk - 1) / kMeas2Chunk;
+    // time ~ rounds of CTAs x work per CTA (1/S of the voxels), +0.5 % per extra range
+    int best = 1;
+    double best_cost = 1e300;
+    for (int s = 1; s <= 64 && s <= chunks; ++s) {
+        const double rounds = (double)((bx * s + slots - 1) / slots);
+        const double cost = rounds / s * (1.0 + 0.005 * (s - 1));
+        if (cost < best_cost - 1e-12) {
+            best_cost = cost;
+            best = s;
+        }
+    }
+    return best;
+}
+
 cudaError_t launch_bwd_meas(const BwdParams &bp, cudaStream_t stream) {
     const int nblk = bp.f.fp / kBlockF;
     const int blocks2 = (bp.num_ant_real + kMeas2Warps - 1) / kMeas2Warps;
-    if (nblk <= 4) {
-        bp_bwd_meas3_kernel<4><<<blocks2, kMeas2Warps * 32, 0, stream>>>(bp);
-    } else if (nblk <= 8) {
-        bp_bwd_meas3_kernel<8><<<blocks2, kMeas2Warps * 32, 0, stream>>>(bp);
+    const dim3 grid3((bp.num_ant_real + kMeas3Warps - 1) / kMeas3Warps, bp.meas_splits);
+    if (nblk <= 8) {
+        if (nblk <= 4)
+            bp_bwd_meas3_kernel<4, kMeas3Warps><<<grid3, kMeas3Warps * 32, 0, stream>>>(bp);
+        else
+            bp_bwd_meas3_kernel<8, kMeas3Warps><<<grid3, kMeas3Warps * 32, 0, stream>>>(bp);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess || bp.meas_splits <= 1) return e;
+        const int64_t n = (int64_t)bp.num_ant_real * bp.num_samples;
+        bwd_meas_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(bp);
     } else if (nblk <= 16) {
         bp_bwd_meas2_kernel<16><<<blocks2, kMeas2Warps * 32, 0, stream>>>(bp);
     } else {

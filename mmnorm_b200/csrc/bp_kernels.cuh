@@ -76,7 +76,9 @@ struct BwdParams {
     int32_t num_samples;       // unpadded F
     int32_t num_ant_real;      // A before padding
     int32_t num_items;         // num_ant_real * (fp / 32): (antenna, 32-sample block) pairs
-    int32_t pad0;
+    int32_t meas_splits;       // voxel ranges of the measurement pass (1: no partial sums)
+    float2 *meas_partial;      // [meas_splits, num_ant_real, num_samples] if meas_splits > 1
+    int64_t vox_per_split;     // voxels per measurement-pass range (a multiple of 512)
 };
 
 cudaError_t launch_bwd_stage(const float *meas, int A, int F, int Fp, double k0, double kd,
@@ -85,6 +87,8 @@ cudaError_t launch_bwd_vox_rec(const BwdParams &bp, float4 *dst, cudaStream_t st
 cudaError_t launch_bwd_pos(const BwdParams &bp, int variant, size_t smem, cudaStream_t stream);
 cudaError_t launch_bwd_pos_reduce(const BwdParams &bp, cudaStream_t stream);
 cudaError_t launch_bwd_meas(const BwdParams &bp, cudaStream_t stream);
+// voxel ranges for the measurement pass: fills the GPU in whole waves of CTAs
+int bwd_meas_splits(int num_ant, int fp, int64_t nvox);
 const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread);
 
 // ---------------------------------------------------------- interpolated mode

@@ -588,7 +588,9 @@ std::atomic<int> g_bwd_variant{0};
 struct BwdPlan {
     int fp, ant_per_stage, tiles, splits, ant_per_split, threads, vpt;
     size_t smem;
-    size_t off_ant, off_meas, off_vox, off_pos, total;
+    size_t off_ant, off_meas, off_vox, off_pos, off_mpart, total;
+    int meas_splits;
+    int64_t vox_per_split;
     const void *fn;
 };
 
@@ -642,6 +644,13 @@ int plan_backward(const mmn_problem *p, BwdPlan *pl) {
     off = align_up(off + (size_t)nvox * 3 * sizeof(float4));
     pl->off_pos = off;
     off = align_up(off + (size_t)pl->tiles * A * 3 * sizeof(float));
+    pl->meas_splits = bwd_meas_splits(A, pl->fp, nvox);
+    const int64_t chunks = (nvox + 511) / 512;
+    pl->vox_per_split = (chunks + pl->meas_splits - 1) / pl->meas_splits * 512;
+    pl->meas_splits = (int)((nvox + pl->vox_per_split - 1) / pl->vox_per_split);
+    pl->off_mpart = off;
+    if (pl->meas_splits > 1)
+        off = align_up(off + (size_t)pl->meas_splits * A * p->num_samples * sizeof(float2));
     pl->total = off;
     return MMN_OK;
 }
@@ -715,6 +724,9 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     bp.num_samples = F;
     bp.num_ant_real = A;
     bp.num_items = A * (pl.fp / kBlockF);
+    bp.meas_splits = pl.meas_splits;
+    bp.meas_partial = reinterpret_cast<float2 *>(ws + pl.off_mpart);
+    bp.vox_per_split = pl.vox_per_split;
     if (grad_pos) {
         if (launch_bwd_stage(p->meas, A, F, pl.fp, f.k0, f.kd, ws + pl.off_meas, stream) !=
             cudaSuccess)
