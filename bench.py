@@ -435,6 +435,26 @@ def ours_arm(args):
         out["plain"]["sfu_bound"] = lane_bounds(updates / (out["plain"]["kernel_ms"] * 1e-3),
                                                 16 / 2)
 
+    numpy_cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the same formula in NumPy (FP64) on all host cores, a seeded voxel sample
+        try:
+            from oracle import numpy_baseline
+            idx = np.sort(np.random.default_rng(5).choice(sc.num_voxels, 8192, replace=False))
+            r = numpy_baseline.time_sample(sc.voxel_centres(idx), sc.antenna_locs,
+                                           np.zeros((1, 3), np.float32), sc.meas,
+                                           sc.wavelength, sc.slope,
+                                           target_seconds=0.75 * args.cpu_seconds)
+            numpy_cpu = {"value": r["updates_per_s"] / 1e9, "unit": UNIT,
+                         "cores": r["workers"], "kind": "port",
+                         "sample": "%d seeded random voxels of the 128^3 grid x all %d antennas "
+                                   "x %d freqs, FP64 NumPy (oracle.full_np) in %d spawn "
+                                   "processes, %.1f s" % (r["voxels"], A, F, r["workers"],
+                                                          r["seconds"])}
+        except Exception as e:  # pragma: no cover
+            numpy_cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": "failed: %s" % str(e)[:200]}
+
     if rank == 0:
         flops = 8.0 * updates          # one complex multiply-add (4 FFMA) per update
         achieved = flops / kern_avg_s / 1e12
@@ -474,6 +494,7 @@ def ours_arm(args):
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "cpu_baseline": cpu,
+            "numpy_baseline": numpy_cpu,
             "adjoint": adjoint,
             "batched": batched,
         }
@@ -522,9 +543,13 @@ def time_adjoint(dev):
                                                    pos_offsets=pos, want_pos=False))
     bwd_p = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
                                                    pos_offsets=pos, want_meas=False))
+    # a loss on the image only (no vote term): one Horner chain in the position pass
+    bwd_i = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, None,
+                                                   pos_offsets=pos))
     return {"workload": sc.name + " (64^3 voxels @3 mm, 64x64 antennas @3 mm, 128 freqs)",
             "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
-            "backward_meas_ms": bwd_m, "backward_pos_ms": bwd_p}
+            "backward_meas_ms": bwd_m, "backward_pos_ms": bwd_p,
+            "backward_image_loss_ms": bwd_i, "backward_image_loss_over_forward": bwd_i / fwd}
 
 
 def time_batched(dev, replays=3):

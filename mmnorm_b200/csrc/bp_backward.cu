@@ -25,10 +25,12 @@
 
 namespace mmn {
 
-// (kappa_j re, re, kappa_j im, im) rows padded to Fp (antenna rows past A and samples past
-// F are zero).
+// Rows padded to Fp (antenna rows past A and samples past F are zero):
+//   layout 0: (kappa_j re, re, kappa_j im, im)  -- the two chains of one voxel
+//   layout 1: (kappa_j re, kappa_j re, kappa_j im, kappa_j im)  -- one chain, voxel pairs
 __global__ void bwd_stage_kernel(const float2 *__restrict__ meas, int A, int F, int Fp,
-                                 int rows, double k0, double kd, float4 *__restrict__ dst) {
+                                 int rows, double k0, double kd, int layout,
+                                 float4 *__restrict__ dst) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)rows * Fp) return;
     const int64_t a = idx / Fp;
@@ -36,7 +38,8 @@ __global__ void bwd_stage_kernel(const float2 *__restrict__ meas, int A, int F, 
     float2 m = make_float2(0.f, 0.f);
     if (a < A && j < F) m = meas[a * F + j];
     const float kap = (float)fma((double)j, kd, k0);
-    dst[idx] = make_float4(kap * m.x, m.x, kap * m.y, m.y);
+    dst[idx] = layout == 0 ? make_float4(kap * m.x, m.x, kap * m.y, m.y)
+                           : make_float4(kap * m.x, kap * m.x, kap * m.y, kap * m.y);
 }
 
 __global__ void bwd_vox_rec_kernel(const BwdParams bp, float4 *__restrict__ dst) {
@@ -135,10 +138,12 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_kernel(const BwdParams bp) {
                     b = sqrt(fma(bx, bx, fma(by, by, bz * bz)));
                 }
                 const double d = f + b + p.ti;
-                // -(e_tx + e_rx): derivative of d with respect to the antenna offset
-                e3[k][0] = -(float)(dx / f + bx / b);
-                e3[k][1] = -(float)(dy / f + by / b);
-                e3[k][2] = -(float)(dz / f + bz / b);
+                // -(e_tx + e_rx): derivative of d with respect to the antenna offset (a
+                // direction: FP32 is ample)
+                const float rf = 1.f / (float)f, rb = mono ? rf : 1.f / (float)b;
+                e3[k][0] = -fmaf((float)dx, rf, (float)bx * rb);
+                e3[k][1] = -fmaf((float)dy, rf, (float)by * rb);
+                e3[k][2] = -fmaf((float)dz, rf, (float)bz * rb);
                 const float2 zz = cis_fp64_phase(-d * p.kd);
                 zr[k] = make_float2(zz.x, zz.x);
                 zi[k] = make_float2(zz.y, zz.y);
@@ -225,6 +230,162 @@ __global__ void bwd_pos_reduce_kernel(const BwdParams bp) {
     for (int t = 0; t < bp.f.num_tiles; ++t)
         s += bp.pos_partial[(size_t)t * bp.f.num_ant * 3 + idx];
     bp.grad_pos[idx] = s;
+}
+
+// Position pass when the loss has no vote term (dL/dW = 0): only c' = sum kappa m p is
+// needed, so the FFMA2 halves carry two voxels' chains (staging layout 1), the forward's
+// voxel-pair arrangement -- half the two-chain kernel's FMA work.
+template <int T, int NT>
+__global__ void __launch_bounds__(NT) bp_bwd_pos_img_kernel(const BwdParams bp) {
+    static_assert(T % 2 == 0, "voxel pairs");
+    constexpr int P = T / 2;
+    const FwdParams &p = bp.f;
+    extern __shared__ __align__(128) unsigned char smem[];
+    Stage st;
+    st.bars = reinterpret_cast<uint64_t *>(smem);
+    st.base = smem + 128;
+    st.nas = p.ant_per_stage;
+    st.esz = 16;
+    st.fp = p.fp;
+    st.stage_bytes = (size_t)st.nas * sizeof(AntRec) + (size_t)st.nas * st.fp * st.esz;
+    float *wsum = reinterpret_cast<float *>(st.base + 2 * st.stage_bytes);  // [NT/32][nas][3]
+    constexpr int NW = NT / 32;
+    const int fp = p.fp;
+    const int tile = blockIdx.x % p.num_tiles;
+    const int split = blockIdx.x / p.num_tiles;
+    const int a_begin = split * p.ant_per_split;
+    const int a_end = min(p.num_ant, a_begin + p.ant_per_split);
+    const int n_chunks = a_end > a_begin ? (a_end - a_begin + st.nas - 1) / st.nas : 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        mbar_init(&st.bars[0], 1);
+        mbar_init(&st.bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n_chunks > 0) st.issue(p, 0, a_begin, a_end);
+        if (n_chunks > 1) st.issue(p, 1, a_begin, a_end);
+    }
+
+    const int64_t rbase = (int64_t)tile * (NT * T) + threadIdx.x;
+    float vx[T], vy[T], vz[T];
+    float2 gi[T];
+#pragma unroll
+    for (int k = 0; k < T; ++k) {
+        const int64_t rel = rbase + (int64_t)k * NT;
+        decode_voxel(p, rel, vx[k], vy[k], vz[k]);
+        const bool ok = rel < p.vox_count;
+        gi[k] = ok ? bp.grad_image[p.vox_start + rel] : make_float2(0.f, 0.f);
+    }
+    const bool mono = *p.mono_flag != 0;
+    const int nblk = fp / kBlockF;
+
+    for (int c = 0; c < n_chunks; ++c) {
+        const int s = c & 1;
+        bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
+        if (!__syncthreads_and(ok)) return;
+        const AntRec *ants = st.ants(s);
+        const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
+        const int a0 = a_begin + c * st.nas;
+        const int na = min(st.nas, a_end - a0);
+
+        for (int a = 0; a < na; ++a) {
+            const AntRec &ar = ants[a];
+            const float4 *m4 = mstage + (size_t)a * fp;
+            float e3[T][3];
+            double d[T];
+            unsigned long long ph[T], stp[T];
+            float2 zr[P], zi[P], nzi[P], cr[P], ci[P];
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const double x = vx[k], y = vy[k], z = vz[k];
+                const double dx = x - ar.tx[0], dy = y - ar.tx[1], dz = z - ar.tx[2];
+                const double f = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+                double b = f, bx = dx, by = dy, bz = dz;
+                if (!mono) {
+                    bx = x - ar.rx[0];
+                    by = y - ar.rx[1];
+                    bz = z - ar.rx[2];
+                    b = sqrt(fma(bx, bx, fma(by, by, bz * bz)));
+                }
+                d[k] = f + b + p.ti;
+                const float rf = 1.f / (float)f, rb = mono ? rf : 1.f / (float)b;
+                e3[k][0] = -fmaf((float)dx, rf, (float)bx * rb);
+                e3[k][1] = -fmaf((float)dy, rf, (float)by * rb);
+                e3[k][2] = -fmaf((float)dz, rf, (float)bz * rb);
+                ph[k] = turns_to_fixed(-d[k] * p.t0);
+                stp[k] = turns_to_fixed(-d[k] * p.tblk);
+            }
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                cis_fp64_phase_pair(-d[2 * q] * p.kd, -d[2 * q + 1] * p.kd, zr[q], zi[q], nzi[q]);
+                cr[q] = ci[q] = make_float2(0.f, 0.f);
+            }
+            for (int b = 0; b < nblk; ++b) {
+                const float4 *mb = m4 + b * kBlockF;
+                float2 hr[P], hi[P];
+                const float4 top = mb[kBlockF - 1];
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    hr[q] = make_float2(top.x, top.y);
+                    hi[q] = make_float2(top.z, top.w);
+                }
+#pragma unroll
+                for (int t = kBlockF - 2; t >= 0; --t) {
+                    const float4 mm = mb[t];
+                    const float2 mr = make_float2(mm.x, mm.y), mi = make_float2(mm.z, mm.w);
+#pragma unroll
+                    for (int q = 0; q < P; ++q) {
+                        const float2 u = __ffma2_rn(hr[q], zr[q], mr);
+                        const float2 w = __ffma2_rn(hr[q], zi[q], mi);
+                        hr[q] = __ffma2_rn(hi[q], nzi[q], u);
+                        hi[q] = __ffma2_rn(hi[q], zr[q], w);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    float2 anr, ani;
+                    fixed_cis(ph[2 * q], anr.x, ani.x);
+                    fixed_cis(ph[2 * q + 1], anr.y, ani.y);
+                    const float2 nani = make_float2(-ani.x, -ani.y);
+                    ph[2 * q] += stp[2 * q];
+                    ph[2 * q + 1] += stp[2 * q + 1];
+                    cr[q] = __ffma2_rn(anr, hr[q], __ffma2_rn(nani, hi[q], cr[q]));
+                    ci[q] = __ffma2_rn(anr, hi[q], __ffma2_rn(ani, hr[q], ci[q]));
+                }
+            }
+            float g3[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const float cpr = (k & 1) ? cr[k / 2].y : cr[k / 2].x;
+                const float cpi = (k & 1) ? ci[k / 2].y : ci[k / 2].x;
+                const float s1 = gi[k].x * cpi - gi[k].y * cpr;  // Im(conj(gI) c')
+#pragma unroll
+                for (int q = 0; q < 3; ++q) g3[q] = fmaf(s1, e3[k][q], g3[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) g3[q] += __shfl_xor_sync(0xffffffffu, g3[q], o);
+            }
+            if (lane == 0) {
+                wsum[(warp * st.nas + a) * 3 + 0] = g3[0];
+                wsum[(warp * st.nas + a) * 3 + 1] = g3[1];
+                wsum[(warp * st.nas + a) * 3 + 2] = g3[2];
+            }
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < na * 3; idx += NT) {
+            float sum = 0.f;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) sum += wsum[w * st.nas * 3 + idx];
+            bp.pos_partial[((size_t)tile * p.num_ant + a0) * 3 + idx] = sum;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
+    }
 }
 
 // --------------------------------------------------------------- measurement pass
@@ -532,6 +693,12 @@ __global__ void bwd_meas_reduce_kernel(const BwdParams bp) {
 }
 
 // -------------------------------------------------------------------- launchers
+const void *bwd_pos_img_kernel_ptr(int *threads, int *voxels_per_thread) {
+    *threads = 256;
+    *voxels_per_thread = 2;
+    return reinterpret_cast<const void *>(&bp_bwd_pos_img_kernel<2, 256>);
+}
+
 const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread) {
     if (variant == 1) {
         *threads = 128;
@@ -544,12 +711,12 @@ const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread
 }
 
 cudaError_t launch_bwd_stage(const float *meas, int A, int F, int Fp, double k0, double kd,
-                             void *dst, cudaStream_t stream) {
+                             int layout, void *dst, cudaStream_t stream) {
     const int nt = 256;
     const int rows = A;
     const int64_t n = (int64_t)rows * Fp;
     bwd_stage_kernel<<<(unsigned)((n + nt - 1) / nt), nt, 0, stream>>>(
-        reinterpret_cast<const float2 *>(meas), A, F, Fp, rows, k0, kd,
+        reinterpret_cast<const float2 *>(meas), A, F, Fp, rows, k0, kd, layout,
         reinterpret_cast<float4 *>(dst));
     return cudaGetLastError();
 }
@@ -562,7 +729,8 @@ cudaError_t launch_bwd_vox_rec(const BwdParams &bp, float4 *dst, cudaStream_t st
 
 cudaError_t launch_bwd_pos(const BwdParams &bp, int variant, size_t smem, cudaStream_t stream) {
     int nt = 0, t = 0;
-    const void *fn = bwd_pos_kernel_ptr(variant, &nt, &t);
+    const void *fn = variant < 0 ? bwd_pos_img_kernel_ptr(&nt, &t)
+                                 : bwd_pos_kernel_ptr(variant, &nt, &t);
     void *args[] = {const_cast<BwdParams *>(&bp)};
     return cudaLaunchKernel(fn, dim3(bp.f.num_tiles * bp.f.num_splits), dim3(nt), args, smem,
                             stream);

@@ -82,7 +82,7 @@ struct BwdParams {
 };
 
 cudaError_t launch_bwd_stage(const float *meas, int A, int F, int Fp, double k0, double kd,
-                             void *dst, cudaStream_t stream);
+                             int layout, void *dst, cudaStream_t stream);
 cudaError_t launch_bwd_vox_rec(const BwdParams &bp, float4 *dst, cudaStream_t stream);
 cudaError_t launch_bwd_pos(const BwdParams &bp, int variant, size_t smem, cudaStream_t stream);
 cudaError_t launch_bwd_pos_reduce(const BwdParams &bp, cudaStream_t stream);
@@ -90,6 +90,8 @@ cudaError_t launch_bwd_meas(const BwdParams &bp, cudaStream_t stream);
 // voxel ranges for the measurement pass: fills the GPU in whole waves of CTAs
 int bwd_meas_splits(int num_ant, int fp, int64_t nvox);
 const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread);
+// position pass for losses without a vote term (launch_bwd_pos with variant -1)
+const void *bwd_pos_img_kernel_ptr(int *threads, int *voxels_per_thread);
 
 // ---------------------------------------------------------- interpolated mode
 struct InterpParams {

@@ -594,10 +594,13 @@ struct BwdPlan {
     const void *fn;
 };
 
-int plan_backward(const mmn_problem *p, BwdPlan *pl) {
+// image_only: the loss has no vote term (grad_vote NULL), so the position pass needs one
+// Horner chain per voxel-antenna and runs the voxel-pair kernel.
+int plan_backward(const mmn_problem *p, bool image_only, BwdPlan *pl) {
     const int A = p->num_antennas;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
-    pl->fn = bwd_pos_kernel_ptr(g_bwd_variant.load(), &pl->threads, &pl->vpt);
+    pl->fn = image_only ? bwd_pos_img_kernel_ptr(&pl->threads, &pl->vpt)
+                        : bwd_pos_kernel_ptr(g_bwd_variant.load(), &pl->threads, &pl->vpt);
     pl->fp = (p->num_samples + kBlockF - 1) / kBlockF * kBlockF;
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
     const int rec = (int)sizeof(AntRec) + pl->fp * 16;
@@ -659,9 +662,10 @@ int plan_backward(const mmn_problem *p, BwdPlan *pl) {
 
 extern "C" size_t mmn_backward_workspace_bytes(const mmn_problem *p) {
     if (check_problem(p, MMN_MODE_MIXED) != MMN_OK) return 0;
-    BwdPlan pl;
-    if (plan_backward(p, &pl) != MMN_OK) return 0;
-    return pl.total;
+    BwdPlan pl, pl_img;
+    if (plan_backward(p, false, &pl) != MMN_OK) return 0;
+    if (plan_backward(p, true, &pl_img) != MMN_OK) return 0;
+    return std::max(pl.total, pl_img.total);
 }
 
 extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
@@ -677,8 +681,9 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     const int A = p->num_antennas;
     const int F = p->num_samples;
     if (A == 0) return MMN_OK;
+    const bool image_only = grad_vote == nullptr;
     BwdPlan pl;
-    rc = plan_backward(p, &pl);
+    rc = plan_backward(p, image_only, &pl);
     if (rc != MMN_OK) return rc;
     if (workspace_bytes < pl.total) return MMN_ERR_WORKSPACE;
     unsigned char *ws = static_cast<unsigned char *>(workspace);
@@ -728,12 +733,13 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     bp.meas_partial = reinterpret_cast<float2 *>(ws + pl.off_mpart);
     bp.vox_per_split = pl.vox_per_split;
     if (grad_pos) {
-        if (launch_bwd_stage(p->meas, A, F, pl.fp, f.k0, f.kd, ws + pl.off_meas, stream) !=
-            cudaSuccess)
+        if (launch_bwd_stage(p->meas, A, F, pl.fp, f.k0, f.kd, image_only ? 1 : 0,
+                             ws + pl.off_meas, stream) != cudaSuccess)
             return MMN_ERR_CUDA;
         if (pl.smem > 48 * 1024)
             cudaFuncSetAttribute(pl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
-        if (launch_bwd_pos(bp, g_bwd_variant.load(), pl.smem, stream) != cudaSuccess)
+        if (launch_bwd_pos(bp, image_only ? -1 : g_bwd_variant.load(), pl.smem, stream) !=
+            cudaSuccess)
             return MMN_ERR_CUDA;
         if (launch_bwd_pos_reduce(bp, stream) != cudaSuccess) return MMN_ERR_CUDA;
     }

@@ -26,9 +26,17 @@ def _stream(device):
     return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 
 
+def _plain(t):
+    """The tensor with torch's lazy conjugate / negative views materialised: the kernels
+    read raw memory through data_ptr(), which ignores those flags."""
+    return t.resolve_conj().resolve_neg() if isinstance(t, torch.Tensor) else t
+
+
 def _need(t, name, dtype, device, shape=None):
     if not isinstance(t, torch.Tensor):
         raise TypeError("%s must be a torch.Tensor" % name)
+    if t.is_conj() or t.is_neg():
+        raise ValueError("%s is a lazy conjugate/negative view; pass t.resolve_conj()" % name)
     if t.device != device:
         raise ValueError("%s is on %s, expected %s" % (name, t.device, device))
     if t.dtype != dtype:
@@ -103,6 +111,7 @@ def backproject(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, waveleng
     ``mode``: 'mixed' (FP64 range/wrap + FP32 recurrence), 'plain' (FP32 sincos per
     sample) or 'interp' (reference interpolated mode; ``meas`` holds range-FFT bins).
     """
+    meas = _plain(meas)
     p = make_problem(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength,
                      slope, fft_spacing, is_ti_radar, pos_offsets)
     dev = meas.device
@@ -126,8 +135,8 @@ def surface_normals(image, vote, filter_percent=0.05, want_raw=False):
     dev = image.device
     shape = tuple(image.shape)
     V = image.numel()
-    img = image.reshape(V)
-    w = vote.reshape(3, V)
+    img = _plain(image).reshape(V)
+    w = _plain(vote).reshape(3, V)
     _need(img, "image", torch.complex64, dev)
     _need(w, "vote", torch.complex64, dev)
     normals = torch.empty((V, 3), dtype=torch.float32, device=dev)
@@ -148,7 +157,7 @@ def surface_normals(image, vote, filter_percent=0.05, want_raw=False):
 def image_max_abs(image, out=None):
     """max |image| as a float32 device tensor of one element (``out`` if given)."""
     dev = image.device
-    img = _need(image.reshape(-1), "image", torch.complex64, dev)
+    img = _need(_plain(image).reshape(-1), "image", torch.complex64, dev)
     if out is None:
         out = torch.empty(1, dtype=torch.float32, device=dev)
     _need(out, "out", torch.float32, dev, (1,))
@@ -163,8 +172,8 @@ def surface_normals_from_max(image, vote, max_abs, filter_percent=0.05, want_raw
     dev = image.device
     shape = tuple(image.shape)
     V = image.numel()
-    img = image.reshape(V)
-    w = vote.reshape(3, V)
+    img = _plain(image).reshape(V)
+    w = _plain(vote).reshape(3, V)
     _need(img, "image", torch.complex64, dev)
     _need(w, "vote", torch.complex64, dev)
     _need(max_abs, "max_abs", torch.float32, dev, (1,))
@@ -213,12 +222,13 @@ def backproject_backward(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas,
                          want_meas=True, want_pos=True):
     """Adjoint of the mixed-precision ``backproject``: (grad_meas complex64 [A, F] or None,
     grad_pos float32 [A, 3] or None) for upstream dL/dI, dL/dW (torch convention)."""
+    meas = _plain(meas)
     p = make_problem(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
                      0.0, is_ti_radar, pos_offsets)
     dev = meas.device
     V = p.num_x * p.num_y * p.num_z
-    gI = grad_image.reshape(V).contiguous() if grad_image is not None else None
-    gW = grad_vote.reshape(3, V).contiguous() if grad_vote is not None else None
+    gI = _plain(grad_image).reshape(V).contiguous() if grad_image is not None else None
+    gW = _plain(grad_vote).reshape(3, V).contiguous() if grad_vote is not None else None
     if gI is None and gW is None:
         gI = torch.zeros(V, dtype=torch.complex64, device=dev)
     A, F = meas.shape
@@ -251,12 +261,17 @@ class BackprojectFunction(torch.autograd.Function):
         ctx.save_for_backward(meas, pos_offsets, x_locs, y_locs, z_locs, antenna_locs,
                               rx_offsets)
         ctx.consts = (wavelength, slope, is_ti_radar)
+        # an output the loss does not use arrives as None, not zeros: without a vote term
+        # the position pass runs one Horner chain instead of two
+        ctx.set_materialize_grads(False)
         return image, vote
 
     @staticmethod
     def backward(ctx, grad_image, grad_vote):
         meas, pos, x, y, z, ant, rxo = ctx.saved_tensors
         wavelength, slope, ti = ctx.consts
+        if grad_image is None and grad_vote is None:
+            return (None,) * 10
         gm, gp = backproject_backward(
             x, y, z, ant, rxo, meas, wavelength, slope,
             grad_image.contiguous() if grad_image is not None else None,
@@ -296,7 +311,7 @@ class BatchPlan:
 
     def __init__(self, objects, items_per_slot=8, want_vote=True):
         lib = _lib.load()
-        self.objects = list(objects)
+        self.objects = [dict(ob, meas=_plain(ob["meas"])) for ob in objects]
         n = len(self.objects)
         dev = self.objects[0]["meas"].device
         self.device = dev

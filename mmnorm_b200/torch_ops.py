@@ -47,7 +47,7 @@ def _(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
 def backproject_backward(x_locs: Tensor, y_locs: Tensor, z_locs: Tensor, antenna_locs: Tensor,
                          rx_offsets: Tensor, meas: Tensor, wavelength: float, slope: float,
                          is_ti_radar: bool, pos_offsets: Optional[Tensor],
-                         grad_image: Tensor, grad_vote: Tensor) -> Tuple[Tensor, Tensor]:
+                         grad_image: Tensor, grad_vote: Optional[Tensor]) -> Tuple[Tensor, Tensor]:
     """Adjoint of the mixed form: (dL/dmeas complex64 [A,F], dL/dpos float32 [A,3])."""
     return ops.backproject_backward(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas,
                                     wavelength, slope, grad_image, grad_vote,
@@ -63,6 +63,7 @@ def _(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
 
 def _setup_context(ctx, inputs, output):
     (x, y, z, ant, rxo, meas, wl, sl, mode, fsp, ti, pos) = inputs
+    ctx.set_materialize_grads(False)
     if mode != "mixed" and (ctx.needs_input_grad[5] or ctx.needs_input_grad[11]):
         raise NotImplementedError("gradients are implemented for mode='mixed' only")
     ctx.save_for_backward(x, y, z, ant, rxo, meas, pos)
@@ -72,13 +73,14 @@ def _setup_context(ctx, inputs, output):
 def _backward(ctx, grad_image, grad_vote):
     x, y, z, ant, rxo, meas, pos = ctx.saved_tensors
     wl, sl, ti = ctx.consts
+    if grad_image is None and grad_vote is None:
+        return (None,) * 12
     V = x.shape[0] * y.shape[0] * z.shape[0]
     gI = grad_image if grad_image is not None else torch.zeros(
         (V,), dtype=torch.complex64, device=meas.device)
-    gW = grad_vote if grad_vote is not None else torch.zeros(
-        (3, V), dtype=torch.complex64, device=meas.device)
+    gW = grad_vote.contiguous() if grad_vote is not None else None   # no vote term
     gm, gp = torch.ops.mmnorm.backproject_backward(x, y, z, ant, rxo, meas, wl, sl, ti, pos,
-                                                   gI.contiguous(), gW.contiguous())
+                                                   gI.contiguous(), gW)
     return (None, None, None, None, None, gm, None, None, None, None, None,
             gp if pos is not None else None)
 

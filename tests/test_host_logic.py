@@ -105,3 +105,18 @@ def test_union_surface_points_are_on_the_boundary():
     in_cyl = (q[:, 0] ** 2 + q[:, 1] ** 2 < 0.04 ** 2 * (1 - 1e-6)) & \
              (np.abs(q[:, 2]) < 0.04 * (1 - 1e-6))
     assert not np.any(in_box & in_cyl)
+
+
+def test_lazy_conjugate_views_are_refused_or_resolved():
+    """The kernels read raw memory; torch's lazy conj/neg views must never reach them."""
+    import pytest
+    import torch
+    from mmnorm_b200 import ops
+    z = torch.tensor([1 + 2j, 3 - 1j], dtype=torch.complex64)
+    zc = z.conj()
+    assert zc.is_conj()
+    with pytest.raises(ValueError):
+        ops._need(zc, "meas", torch.complex64, z.device)
+    r = ops._plain(zc)
+    assert not r.is_conj() and torch.equal(r, torch.conj_physical(z))
+    ops._need(r, "meas", torch.complex64, z.device)
