@@ -190,6 +190,38 @@ int mmn_normals_from_max(int64_t num_voxels, const float *image, const float *vo
                          uint8_t *mask, float *raw, cudaStream_t stream);
 
 /*
+ * Connected components (6-connectivity) of a voxel mask, as
+ * _find_connected_components does with cc3d.connected_components(mask, connectivity=6)
+ * (src/data_processing/sdf.py:94-120).  mask: uint8 [V] (1 = voxel with a valid normal).
+ * root: int32 [V], the smallest flat index in the voxel's component (-1 outside the mask);
+ * count: int32 [V], the component's voxel count at its root index (0 elsewhere).  The
+ * root is a canonical label: it does not depend on the order of the GPU's unions.
+ * Needs mmn_components_workspace_bytes() of workspace (the status word).
+ */
+size_t mmn_components_workspace_bytes(int64_t num_voxels);
+int mmn_components(int32_t num_x, int32_t num_y, int32_t num_z, const uint8_t *mask,
+                   int32_t *root, int32_t *count, void *workspace, size_t workspace_bytes,
+                   cudaStream_t stream);
+
+/*
+ * Relative signed distance field of one component by breadth-first integration of the
+ * normals (_construct_rsdf_components, src/data_processing/sdf.py:122-224): from voxel
+ * `seed` (rsdf 0), every voxel of the component with root `comp_root` receives
+ * rsdf[cell] + dot(step * dx, normal[voxel]) from the cell that enqueues it in the
+ * reference's FIFO order (neighbours -x, +y, +x, -y, +z, -z), bit for bit.
+ * normals: float64 [V, 3] (NaN x-component = no normal); rsdf: float64 [V], written only
+ * on the component's voxels (the caller initialises the rest, e.g. to NaN).
+ * *visited_count (may be NULL) receives the number of voxels reached.  Synchronises
+ * `stream` once per search level (the next level's size decides the launch).
+ * Grids up to 357,913,941 voxels.
+ */
+size_t mmn_rsdf_workspace_bytes(int32_t num_x, int32_t num_y, int32_t num_z);
+int mmn_rsdf_component(int32_t num_x, int32_t num_y, int32_t num_z, const double *normals,
+                       const int32_t *root, int32_t comp_root, int32_t seed, double dx,
+                       double *rsdf, int64_t *visited_count, void *workspace,
+                       size_t workspace_bytes, cudaStream_t stream);
+
+/*
  * Drop-in for the reference kernel launch `cuda_image`
  * (src/data_processing/cuda/imaging_gpu.cu:12-21, launched at py_image_gpu.py:189-199):
  * same arguments in the same order and meaning (SoA measurements, float scalars,

@@ -83,6 +83,13 @@ SIGNATURES = [
     ("mmn_normals_workspace_bytes", _SZ, [ctypes.c_int64]),
     ("mmn_normals", _I, [ctypes.c_int64, _P, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     ("mmn_image_max_abs", _I, [ctypes.c_int64, _P, _P, _P]),
+    ("mmn_components_workspace_bytes", _SZ, [ctypes.c_int64]),
+    ("mmn_components", _I, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P,
+                            _SZ, _P]),
+    ("mmn_rsdf_workspace_bytes", _SZ, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    ("mmn_rsdf_component", _I, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                                ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _P, _P, _P,
+                                _SZ, _P]),
     ("mmn_normals_from_max", _I, [ctypes.c_int64, _P, _P, _P, _F, _P, _P, _P, _P]),
     ("mmn_cuda_image_workspace_bytes", _SZ, [_I, _I, _I]),
     ("mmn_cuda_image_workspace_bytes_for", _SZ, [_I, _I, _I, _I, _I, _I, _I, _I]),
