@@ -222,6 +222,49 @@ int mmn_rsdf_component(int32_t num_x, int32_t num_y, int32_t num_z, const double
                        size_t workspace_bytes, cudaStream_t stream);
 
 /*
+ * Channels simulated from isosurfaces of the RSDF (_simulate_channels,
+ * src/data_processing/isosurface_optimization.py:116-208, with the ray marching of
+ * src/data_processing/cuda/ray_tracing_kernel.cu): for every offset set t and antenna a,
+ * width x height rays from the antenna over +-width_fov / +-height_fov degrees march each
+ * component's grid (rsdf - taus[t][c]); every hit, refined by one trilinear step, adds
+ * exp(j 2 pi d f_k / c) (d the round trip plus range_offset) at every frequency
+ * f_k / c = f0_over_c + k * df_over_c, summed over the components.
+ * grids: float32 [num_comp][res_x][res_y][res_z], -50 where undefined.  bbox: min x, y, z,
+ * max x, y, z (float32, as the marching kernel receives them); voxel_size and lower: the
+ * FP32 voxel size and lower corner the refinement step uses.
+ */
+typedef struct mmn_iso_scene {
+    const float *grids;
+    int32_t num_comp;
+    int32_t res_x, res_y, res_z;
+    float bbox[6];
+    float voxel_size;
+    float lower[3];
+    int32_t width, height;
+    float width_fov, height_fov;
+    double range_offset;
+    double f0_over_c, df_over_c;
+    int32_t num_wl;
+    int32_t reserved;
+} mmn_iso_scene;
+
+/* taus: float32 [num_sets][num_comp]; rx_locs: float64 [num_antennas][3]; rx_dirs: float32
+ * [num_antennas][3]; channels: complex64 [num_sets][num_antennas][num_wl].  Sets x antennas
+ * <= 65535 per call. */
+size_t mmn_iso_channels_workspace_bytes(const mmn_iso_scene *scene, int32_t num_sets,
+                                        int32_t num_antennas);
+int mmn_iso_channels(const mmn_iso_scene *scene, const float *taus, int32_t num_sets,
+                     const double *rx_locs, const float *rx_dirs, int32_t num_antennas,
+                     float *channels, void *workspace, size_t workspace_bytes,
+                     cudaStream_t stream);
+/* The rough march of one antenna's rays on component `comp` at offset `tau` (the
+ * reference extension's ray_matching outputs): rough hit point, hit voxel index (both -1
+ * for no hit) and ray direction, float32 [width * height][3] each. */
+int mmn_iso_march(const mmn_iso_scene *scene, int32_t comp, float tau, const double *rx_loc,
+                  const float *rx_dir, float *rough, float *voxel, float *direction,
+                  cudaStream_t stream);
+
+/*
  * Drop-in for the reference kernel launch `cuda_image`
  * (src/data_processing/cuda/imaging_gpu.cu:12-21, launched at py_image_gpu.py:189-199):
  * same arguments in the same order and meaning (SoA measurements, float scalars,

@@ -59,6 +59,20 @@ class MmnProblem(ctypes.Structure):
     ]
 
 
+class MmnIsoScene(ctypes.Structure):
+    """Mirror of ``mmn_iso_scene`` (include/mmnorm_b200.h)."""
+
+    _fields_ = [
+        ("grids", ctypes.c_void_p), ("num_comp", ctypes.c_int32),
+        ("res_x", ctypes.c_int32), ("res_y", ctypes.c_int32), ("res_z", ctypes.c_int32),
+        ("bbox", ctypes.c_float * 6), ("voxel_size", ctypes.c_float),
+        ("lower", ctypes.c_float * 3), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+        ("width_fov", ctypes.c_float), ("height_fov", ctypes.c_float),
+        ("range_offset", ctypes.c_double), ("f0_over_c", ctypes.c_double),
+        ("df_over_c", ctypes.c_double), ("num_wl", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+
 # (name, restype, argtypes) of every entry point in include/mmnorm_b200.h
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -83,6 +97,10 @@ SIGNATURES = [
     ("mmn_normals_workspace_bytes", _SZ, [ctypes.c_int64]),
     ("mmn_normals", _I, [ctypes.c_int64, _P, _P, _F, _P, _P, _P, _P, _SZ, _P]),
     ("mmn_image_max_abs", _I, [ctypes.c_int64, _P, _P, _P]),
+    ("mmn_iso_channels_workspace_bytes", _SZ, [ctypes.POINTER(MmnIsoScene), _I32, _I32]),
+    ("mmn_iso_channels", _I, [ctypes.POINTER(MmnIsoScene), _P, _I32, _P, _P, _I32, _P, _P, _SZ,
+                              _P]),
+    ("mmn_iso_march", _I, [ctypes.POINTER(MmnIsoScene), _I32, _F, _P, _P, _P, _P, _P, _P]),
     ("mmn_components_workspace_bytes", _SZ, [ctypes.c_int64]),
     ("mmn_components", _I, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P,
                             _SZ, _P]),

@@ -12,7 +12,11 @@ Two things are built here, both as checkers, never as the product:
        x86-64-v3 host, and the unused boost libraries are not linked;
      * ``imaging_gpu.cubin`` / ``surface_normal_est.cubin``: the reference CUDA kernels
        (src/data_processing/cuda/imaging_gpu.cu, surface_normal_est.cu) compiled
-       unmodified for sm_100a, to be launched by ``oracle/ref_cuda.py``.
+       unmodified for sm_100a, to be launched by ``oracle/ref_cuda.py``;
+     * ``raytrace/ray_tracing_ref.so``: the reference's ray-marching extension
+       (src/data_processing/cpp/ray_tracing.cpp + src/data_processing/cuda/
+       ray_tracing_kernel.cu, the two sources its setup.py lists) compiled unmodified for
+       sm_100a with torch's extension builder, imported by ``oracle/iso_oracle.py``.
 
 Outputs under ``oracle/_ref`` and ``oracle/_build`` are git-ignored build products.
 Usage: ``python oracle/build.py [--ref-root PATH]``.
@@ -86,6 +90,21 @@ def build_ref(ref_root: str = DEFAULT_REF_ROOT, force: bool = False) -> dict:
             _run([NVCC, "-cubin", "-gencode", "arch=compute_100a,code=sm_100a",
                   "-o", out, src])
         built[name] = out
+
+    rt_cpp = os.path.join(cpp_dir, "ray_tracing.cpp")
+    rt_cu = os.path.join(cu_dir, "ray_tracing_kernel.cu")
+    if os.path.exists(rt_cpp) and os.path.exists(rt_cu):
+        out_dir = os.path.join(REF_OUT, "raytrace")
+        so = os.path.join(out_dir, "ray_tracing_ref.so")
+        if force or _stale(so, [rt_cpp, rt_cu]):
+            os.makedirs(out_dir, exist_ok=True)
+            os.environ["TORCH_CUDA_ARCH_LIST"] = ""   # the -gencode below decides the arch
+            from torch.utils import cpp_extension
+            cpp_extension.load(name="ray_tracing_ref", sources=[rt_cpp, rt_cu],
+                               extra_cuda_cflags=["-gencode", "arch=compute_100a,code=sm_100a",
+                                                  "-O3"],
+                               extra_cflags=["-O2"], build_directory=out_dir, verbose=False)
+        built["ray_tracing"] = so
     return built
 
 
