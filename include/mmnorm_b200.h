@@ -265,6 +265,32 @@ int mmn_iso_march(const mmn_iso_scene *scene, int32_t comp, float tau, const dou
                   cudaStream_t stream);
 
 /*
+ * Raw 77 GHz ADC samples (GenericLoader.load_radar_files, src/utils/generic_loader.py:
+ * 521-535): raw holds little-endian int16, 8 per sample (I of lanes 0-3, then Q of lanes
+ * 0-3); out: complex64 [num_samples][4] (the int16 values are exact in FP32).
+ */
+int mmn_adc_unpack(const int16_t *raw, int64_t num_samples, float *out, cudaStream_t stream);
+
+/*
+ * The antenna position of every radar frame (ImageProcessor.correlate_locs_and_meas,
+ * src/data_processing/image_processor.py:74-154): per row (radar file) r and frame j, the
+ * trajectory (times ascending [num_points], traj [num_points][dim], 3 <= dim <= 8) is
+ * interpolated linearly at created[r] + j * frame_dt as scipy's interp1d does; the frame is
+ * kept unless its time is outside the trajectory, it lies within `threshold` of a frame
+ * kept earlier in the same row (j > 0; with no frame kept yet in the row, frames j > 0 are
+ * dropped, as the reference's minimum over an empty list raises), or the row's file holds
+ * fewer than j * frame_stride + samples samples (available[r]; -1 skips the row).
+ * optitrack != 0 applies the optitrack axis change (-x, z, y) to kept positions.
+ * loc_out: float64 [num_rows][num_frames][optitrack ? 3 : dim]; keep: uint8
+ * [num_rows][num_frames]; scratch: int32 [num_rows][num_frames].
+ */
+int mmn_correlate_poses(const double *times, const double *traj, int64_t num_points,
+                        int32_t dim, const double *created, const int64_t *available,
+                        int32_t num_rows, int32_t num_frames, double frame_dt, double threshold,
+                        int64_t frame_stride, int64_t samples, int32_t optitrack,
+                        double *loc_out, uint8_t *keep, int32_t *scratch, cudaStream_t stream);
+
+/*
  * Drop-in for the reference kernel launch `cuda_image`
  * (src/data_processing/cuda/imaging_gpu.cu:12-21, launched at py_image_gpu.py:189-199):
  * same arguments in the same order and meaning (SoA measurements, float scalars,

@@ -101,6 +101,10 @@ SIGNATURES = [
     ("mmn_iso_channels", _I, [ctypes.POINTER(MmnIsoScene), _P, _I32, _P, _P, _I32, _P, _P, _SZ,
                               _P]),
     ("mmn_iso_march", _I, [ctypes.POINTER(MmnIsoScene), _I32, _F, _P, _P, _P, _P, _P, _P]),
+    ("mmn_adc_unpack", _I, [_P, ctypes.c_int64, _P, _P]),
+    ("mmn_correlate_poses", _I, [_P, _P, ctypes.c_int64, _I32, _P, _P, _I32, _I32,
+                                 ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                                 ctypes.c_int64, _I32, _P, _P, _P, _P]),
     ("mmn_components_workspace_bytes", _SZ, [ctypes.c_int64]),
     ("mmn_components", _I, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P,
                             _SZ, _P]),
