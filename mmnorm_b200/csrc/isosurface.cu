@@ -19,10 +19,10 @@
 // exp(j 2 pi d f_k / c) from an exact fixed-point phase per (hit, wavelength) and the
 // hardware sincos on the wrapped angle (f_k uniform, f_k = c / lambda_k).
 //
-// Work item = (offset set t, antenna a); grid = (ray blocks, items).  A block marches 256
-// rays through every component, collects its hits in ray order, writes its partial channel
-// [K] and hit count; a second kernel adds the blocks' partials in block order (FP64) --
-// deterministic run to run.
+// Work item = (offset set t, antenna a); grid = (ray blocks, items).  A block takes every
+// blocks-per-item-th tile of 256 rays, marches them through every component, collects the
+// hits in ray order and adds them to its partial channel [K]; a second kernel adds the
+// blocks' partials in block order (FP64) -- deterministic run to run.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -65,35 +65,48 @@ __device__ __forceinline__ float vlen(const float x, const float y, const float 
     return sqrtf(powf(x, 2) + powf(y, 2) + powf(z, 2));
 }
 
-// ray direction of pixel (px, py) from the antenna's view frame
-__device__ void ray_direction(const IsoParams &p, int px, int py, float rdx, float rdy, float rdz,
-                              float &dx, float &dy, float &dz) {
+// the antenna's view frame (w along the antenna direction, u = up x w, v = w x u) and the
+// field of view in radians: the same for every ray of an antenna, formed once per block
+struct RayBasis {
+    float w_x, w_y, w_z, u_x, u_y, u_z, v_x, v_y, v_z, horiz_fov, vert_fov;
+};
+
+__device__ RayBasis ray_basis(const IsoParams &p, float rdx, float rdy, float rdz) {
+    RayBasis b;
     const float up_x = 1, up_y = 0, up_z = 0;
-    const float vert_fov = deg_to_rad(p.height_fov);
-    const float horiz_fov = deg_to_rad(p.width_fov);
-    const float w_x = (rdx) / vlen(rdx, rdy, rdz);
-    const float w_y = (rdy) / vlen(rdx, rdy, rdz);
-    const float w_z = (rdz) / vlen(rdx, rdy, rdz);
-    const float cuw_x = up_y * w_z - up_z * w_y;
-    const float cuw_y = up_z * w_x - up_x * w_z;
-    const float cuw_z = up_x * w_y - up_y * w_x;
-    const float u_x = (cuw_x) / vlen(cuw_x, cuw_y, cuw_z);
-    const float u_y = (cuw_y) / vlen(cuw_x, cuw_y, cuw_z);
-    const float u_z = (cuw_z) / vlen(cuw_x, cuw_y, cuw_z);
-    const float v_x = w_y * u_z - w_z * u_y;
-    const float v_y = w_z * u_x - w_x * u_z;
-    const float v_z = w_x * u_y - w_y * u_x;
+    b.vert_fov = deg_to_rad(p.height_fov);
+    b.horiz_fov = deg_to_rad(p.width_fov);
+    b.w_x = (rdx) / vlen(rdx, rdy, rdz);
+    b.w_y = (rdy) / vlen(rdx, rdy, rdz);
+    b.w_z = (rdz) / vlen(rdx, rdy, rdz);
+    const float cuw_x = up_y * b.w_z - up_z * b.w_y;
+    const float cuw_y = up_z * b.w_x - up_x * b.w_z;
+    const float cuw_z = up_x * b.w_y - up_y * b.w_x;
+    b.u_x = (cuw_x) / vlen(cuw_x, cuw_y, cuw_z);
+    b.u_y = (cuw_y) / vlen(cuw_x, cuw_y, cuw_z);
+    b.u_z = (cuw_z) / vlen(cuw_x, cuw_y, cuw_z);
+    b.v_x = b.w_y * b.u_z - b.w_z * b.u_y;
+    b.v_y = b.w_z * b.u_x - b.w_x * b.u_z;
+    b.v_z = b.w_x * b.u_y - b.w_y * b.u_x;
+    return b;
+}
+
+// ray direction of pixel (px, py)
+__device__ void ray_direction(const IsoParams &p, const RayBasis &b, int px, int py, float &dx,
+                              float &dy, float &dz) {
+    const float horiz_fov = b.horiz_fov, vert_fov = b.vert_fov;
     // the angle is formed in double (a float plus 0.5) and narrowed, as the reference does
     const float horiz_angle = -horiz_fov + (horiz_fov*2) * (__int2float_rd(px) + 0.5)/ __int2float_rd(p.width);
     const float vert_angle = -vert_fov + (vert_fov*2) * (__int2float_rd(py) + 0.5)/ __int2float_rd(p.height);
     const float view_plane_x = tan(horiz_angle);
     const float view_plane_y = tan(vert_angle);
-    const float s_x = view_plane_x * u_x + view_plane_y * v_x - w_x;
-    const float s_y = view_plane_x * u_y + view_plane_y * v_y - w_y;
-    const float s_z = view_plane_x * u_z + view_plane_y * v_z - w_z;
-    dx = s_x / vlen(s_x, s_y, s_z);
-    dy = s_y / vlen(s_x, s_y, s_z);
-    dz = s_z / vlen(s_x, s_y, s_z);
+    const float s_x = view_plane_x * b.u_x + view_plane_y * b.v_x - b.w_x;
+    const float s_y = view_plane_x * b.u_y + view_plane_y * b.v_y - b.w_y;
+    const float s_z = view_plane_x * b.u_z + view_plane_y * b.v_z - b.w_z;
+    const float len = vlen(s_x, s_y, s_z);
+    dx = s_x / len;
+    dy = s_y / len;
+    dz = s_z / len;
 }
 
 __device__ __forceinline__ bool inside_box(const IsoParams &p, float x, float y, float z) {
@@ -258,7 +271,7 @@ __global__ void __launch_bounds__(kIsoThreads) iso_channel_kernel(const IsoParam
     const int ntiles = (npix + kIsoThreads - 1) / kIsoThreads;
     const float eye_x = (float)p.rx_locs[3 * a], eye_y = (float)p.rx_locs[3 * a + 1],
                 eye_z = (float)p.rx_locs[3 * a + 2];
-    const float rdx = p.rx_dirs[3 * a], rdy = p.rx_dirs[3 * a + 1], rdz = p.rx_dirs[3 * a + 2];
+    const RayBasis basis = ray_basis(p, p.rx_dirs[3 * a], p.rx_dirs[3 * a + 1], p.rx_dirs[3 * a + 2]);
     const int64_t ncell = (int64_t)p.res_x * p.res_y * p.res_z;
     const int64_t bslot = (int64_t)item * p.blocks_per_item + blockIdx.x;
     float2 *dst = p.partial + bslot * p.num_wl;
@@ -269,7 +282,7 @@ __global__ void __launch_bounds__(kIsoThreads) iso_channel_kernel(const IsoParam
     for (int tile = blockIdx.x; tile < ntiles; tile += p.blocks_per_item) {
         const int pixel = tile * kIsoThreads + threadIdx.x;
         float dx = 0.f, dy = 0.f, dz = 0.f;
-        if (pixel < npix) ray_direction(p, pixel % p.width, pixel / p.width, rdx, rdy, rdz, dx, dy, dz);
+        if (pixel < npix) ray_direction(p, basis, pixel % p.width, pixel / p.width, dx, dy, dz);
         for (int c = 0; c < p.num_comp; ++c) {
             const float *g = p.grids + (int64_t)c * ncell;
             const float tau = p.taus[(int64_t)t * p.num_comp + c];
@@ -354,8 +367,9 @@ __global__ void iso_march_debug_kernel(const IsoParams p, int comp, float tau, i
     const int pixel = blockIdx.x * blockDim.x + threadIdx.x;
     if (pixel >= p.width * p.height) return;
     float dx, dy, dz;
-    ray_direction(p, pixel % p.width, pixel / p.width, p.rx_dirs[3 * ant], p.rx_dirs[3 * ant + 1],
-                  p.rx_dirs[3 * ant + 2], dx, dy, dz);
+    const RayBasis basis =
+        ray_basis(p, p.rx_dirs[3 * ant], p.rx_dirs[3 * ant + 1], p.rx_dirs[3 * ant + 2]);
+    ray_direction(p, basis, pixel % p.width, pixel / p.width, dx, dy, dz);
     const int64_t ncell = (int64_t)p.res_x * p.res_y * p.res_z;
     float hx = -1, hy = -1, hz = -1, vx = -1, vy = -1, vz = -1;
     if (!march(p, p.grids + comp * ncell, tau, (float)p.rx_locs[3 * ant],
