@@ -99,12 +99,16 @@ def build_ref(ref_root: str = DEFAULT_REF_ROOT, force: bool = False) -> dict:
         if force or _stale(so, [rt_cpp, rt_cu]):
             os.makedirs(out_dir, exist_ok=True)
             os.environ["TORCH_CUDA_ARCH_LIST"] = ""   # the -gencode below decides the arch
-            from torch.utils import cpp_extension
-            cpp_extension.load(name="ray_tracing_ref", sources=[rt_cpp, rt_cu],
-                               extra_cuda_cflags=["-gencode", "arch=compute_100a,code=sm_100a",
-                                                  "-O3"],
-                               extra_cflags=["-O2"], build_directory=out_dir, verbose=False)
-        built["ray_tracing"] = so
+            try:
+                from torch.utils import cpp_extension
+                cpp_extension.load(name="ray_tracing_ref", sources=[rt_cpp, rt_cu],
+                                   extra_cuda_cflags=["-gencode",
+                                                      "arch=compute_100a,code=sm_100a", "-O3"],
+                                   extra_cflags=["-O2"], build_directory=out_dir, verbose=False)
+            except Exception as e:  # the checker is optional: its tests skip without it
+                print("reference ray-marching extension not built: %s" % str(e)[:300])
+        if os.path.exists(so):
+            built["ray_tracing"] = so
     return built
 
 
