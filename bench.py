@@ -364,11 +364,14 @@ def ours_arm(args):
     # end to end through the public API: pinned host inputs -> device -> image + normals
     # -> pinned host outputs, every step
     e2e = None
-    if rank == 0 and not args.no_e2e:
+    if not args.no_e2e:
+        # every rank: its slab's inputs from pinned host memory, the step, its image and
+        # normals back to pinned host memory; the mask's max|I| all-reduced as in the step
         h_meas = torch.empty(meas.shape, dtype=meas.dtype, pin_memory=True)
         h_meas.copy_(torch.as_tensor(sc.meas))
         h_ant = torch.as_tensor(sc.antenna_locs).pin_memory()
-        h_axes = [torch.as_tensor(a).pin_memory() for a in (sc.x_locs, sc.y_locs, sc.z_locs)]
+        h_axes = [xs.cpu().pin_memory()] + [torch.as_tensor(a).pin_memory()
+                                            for a in (sc.y_locs, sc.z_locs)]
         h_rxo = torch.zeros((1, 3), dtype=torch.float32).pin_memory()
         h_img = torch.empty(V, dtype=torch.complex64, pin_memory=True)
         h_nrm = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
@@ -382,27 +385,35 @@ def ours_arm(args):
             d_rxo = h_rxo.to(dev, non_blocking=True)
             img, vote = ops.backproject(*d_axes, d_ant, d_rxo, d_meas, sc.wavelength, sc.slope,
                                         mode="mixed")
-            normals, mask = ops.surface_normals(img, vote, 0.05)
+            mx = ops.image_max_abs(img)
+            if world > 1:
+                dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            normals, mask = ops.surface_normals_from_max(img, vote, mx, 0.05)
             h_img.copy_(img.reshape(-1), non_blocking=True)
             h_nrm.copy_(normals.reshape(-1, 3), non_blocking=True)
             torch.cuda.synchronize()
 
         e2e_step()
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
+        barrier()
         s0.record(stream)
         for _ in range(n_e2e):
             e2e_step()
         s1.record(stream)
-        torch.cuda.synchronize()
+        barrier()
         ems = s0.elapsed_time(s1) / n_e2e
+        if world > 1:
+            et = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+            ems = float(et.item())
         h2d = (h_meas.numel() * 8 + h_ant.numel() * 4 + sum(a.numel() for a in h_axes) * 4
                + h_rxo.numel() * 4)
         d2h = h_img.numel() * 8 + h_nrm.numel() * 4
-        e2e = {"value": updates / (ems * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": ems,
-               "path": "pinned host -> ops.backproject + ops.surface_normals (C ABI) -> "
-                       "pinned host image + unit normals"}
+        e2e = {"value": world * updates / (ems * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": h2d * world, "d2h_bytes_per_step": d2h * world,
+               "ms_per_step": ems,
+               "path": "pinned host -> ops.backproject + image_max_abs (+ all-reduce) + "
+                       "surface_normals_from_max (C ABI) -> pinned host image + unit normals"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

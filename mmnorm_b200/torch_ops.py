@@ -12,7 +12,7 @@ Each operator calls the same C ABI as ``mmnorm_b200.ops``; nothing here computes
 """
 from __future__ import annotations
 
-from typing import Optional, Tuple
+from typing import List, Optional, Tuple
 
 import torch
 from torch import Tensor
@@ -109,3 +109,30 @@ def _(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
             meas.new_empty((3,) + shp, dtype=torch.complex64),
             meas.new_empty(shp + (3,), dtype=torch.float32),
             meas.new_empty(shp, dtype=torch.bool))
+
+
+@torch.library.custom_op("mmnorm::backproject_batched", mutates_args=())
+def backproject_batched(x_locs: List[Tensor], y_locs: List[Tensor], z_locs: List[Tensor],
+                        antenna_locs: List[Tensor], rx_offsets: List[Tensor], meas: List[Tensor],
+                        wavelength: List[float], slope: List[float], is_ti_radar: List[bool],
+                        items_per_slot: int) -> Tuple[List[Tensor], List[Tensor]]:
+    """Many objects in one persistent launch (mixed form): images and votes per object."""
+    objs = [dict(x_locs=x_locs[o], y_locs=y_locs[o], z_locs=z_locs[o],
+                 antenna_locs=antenna_locs[o], rx_offsets=rx_offsets[o], meas=meas[o],
+                 wavelength=wavelength[o], slope=slope[o], is_ti_radar=is_ti_radar[o])
+            for o in range(len(meas))]
+    plan = ops.BatchPlan(objs, items_per_slot=items_per_slot)
+    plan.run()
+    res = plan.results()
+    return [r[0] for r in res], [r[1] for r in res]
+
+
+@backproject_batched.register_fake
+def _(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope, is_ti_radar,
+      items_per_slot):
+    imgs, votes = [], []
+    for o in range(len(meas)):
+        shp = (x_locs[o].shape[0], y_locs[o].shape[0], z_locs[o].shape[0])
+        imgs.append(meas[o].new_empty(shp, dtype=torch.complex64))
+        votes.append(meas[o].new_empty((3,) + shp, dtype=torch.complex64))
+    return imgs, votes

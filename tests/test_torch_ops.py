@@ -27,6 +27,11 @@ def test_operators_registered_with_fake_shapes():
         gm, gp = torch.ops.mmnorm.backproject_backward(x, y, z, ant, rxo, m, 4e-3, 1e8, False,
                                                        None, i, v)
         assert gm.shape == (7, 32) and gp.shape == (7, 3)
+        imgs, votes = torch.ops.mmnorm.backproject_batched(
+            [x, y], [y, z], [z, x], [ant, ant], [rxo, rxo], [m, m], [4e-3, 4e-3], [1e8, 1e8],
+            [False, True], 8)
+        assert [tuple(t.shape) for t in imgs] == [(4, 5, 6), (5, 6, 4)]
+        assert tuple(votes[1].shape) == (3, 5, 6, 4)
 
 
 @pytest.mark.gpu
@@ -64,3 +69,18 @@ def test_operators_match_ops_and_autograd(cuda_dev):
         loss(img, vote).backward()
         grads.append((meas.grad.clone(), pos.grad.clone()))
     assert torch.equal(grads[0][0], grads[1][0]) and torch.equal(grads[0][1], grads[1][1])
+
+    # the batched operator: the same results as a BatchPlan over the same objects
+    objs = [dict(x_locs=x, y_locs=y, z_locs=z, antenna_locs=ant, rx_offsets=rxo,
+                 meas=t(sc.meas), wavelength=sc.wavelength, slope=sc.slope),
+            dict(x_locs=x[:5].contiguous(), y_locs=y, z_locs=z, antenna_locs=ant[:30].contiguous(),
+                 rx_offsets=rxo, meas=t(sc.meas[:30]), wavelength=sc.wavelength, slope=sc.slope)]
+    plan = ops.BatchPlan(objs, items_per_slot=8)
+    plan.run()
+    ref = plan.results()
+    imgs, votes = torch.ops.mmnorm.backproject_batched(
+        [o["x_locs"] for o in objs], [o["y_locs"] for o in objs], [o["z_locs"] for o in objs],
+        [o["antenna_locs"] for o in objs], [o["rx_offsets"] for o in objs],
+        [o["meas"] for o in objs], [sc.wavelength] * 2, [sc.slope] * 2, [False, False], 8)
+    for (ri, rv), gi, gv in zip(ref, imgs, votes):
+        assert torch.equal(ri, gi) and torch.equal(rv, gv)
