@@ -456,9 +456,9 @@ __global__ void __launch_bounds__(kMeasThreads) bp_bwd_meas_kernel(const BwdPara
 constexpr int kMeas2Warps = 8;
 constexpr int kMeas2Chunk = 512;  // voxel records per shared-memory chunk (24 KB)
 
-__device__ __forceinline__ void warp_transpose_reduce32(float (&v)[kBlockF]) {
+__device__ __forceinline__ void warp_transpose_reduce32(float (&v)[kBlockF], int first_level = 0) {
 #pragma unroll
-    for (int level = 0; level < 5; ++level) {
+    for (int level = first_level; level < 5; ++level) {
         const int half = 16 >> level;
 #pragma unroll
         for (int i = 0; i < half; ++i) v[i] += __shfl_xor_sync(0xffffffffu, v[i + half], half);
@@ -555,41 +555,70 @@ __global__ void __launch_bounds__(kMeas2Warps * 32) bp_bwd_meas2_kernel(const Bw
 // slot - lowest set bit), so only the ancestor path is live; each pair is folded into one
 // scalar slot (the two voxels' sum) as soon as it exists, and one transpose-reduce then
 // serves 64 voxels.
+template <int G>
 struct PairSteps {
-    float2 wr[5], wi[5], nwi[5];  // per-half step conj(z)^(2^k), conjugated where lane bit k is set
+    // per voxel pair g and half: step conj(z)^(2^k), conjugated where lane bit k is set
+    float2 wr[G][5], wi[G][5], nwi[G][5];
 };
 
 __host__ __device__ constexpr int dfs_child_bits(int i) { return i == 0 ? 5 : (i & 1 ? 0 : 1 + dfs_child_bits(i >> 1)); }
 
-template <int I>
-__device__ __forceinline__ void meas_dfs(float2 r, float2 m, const PairSteps &w,
-                                         float (&sr)[kBlockF], float (&si)[kBlockF]);
+template <int I, int G>
+__device__ __forceinline__ void meas_dfs(const float2 (&r)[G], const float2 (&m)[G],
+                                         const PairSteps<G> &w, float (&sr)[kBlockF],
+                                         float (&si)[kBlockF]);
 
 // children of slot I are I + 2^k for k below I's lowest set bit, visited from the top bit down
-template <int I, int K>
-__device__ __forceinline__ void meas_dfs_children(float2 r, float2 m, const PairSteps &w,
-                                                  float (&sr)[kBlockF], float (&si)[kBlockF]) {
+template <int I, int K, int G>
+__device__ __forceinline__ void meas_dfs_children(const float2 (&r)[G], const float2 (&m)[G],
+                                                  const PairSteps<G> &w, float (&sr)[kBlockF],
+                                                  float (&si)[kBlockF]) {
     if constexpr (K > 0) {
         constexpr int k = K - 1;
-        const float2 cr = __ffma2_rn(m, w.nwi[k], __fmul2_rn(r, w.wr[k]));
-        const float2 cm = __ffma2_rn(r, w.wi[k], __fmul2_rn(m, w.wr[k]));
-        meas_dfs<I + (1 << k)>(cr, cm, w, sr, si);
-        meas_dfs_children<I, K - 1>(r, m, w, sr, si);
+        float2 cr[G], cm[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            cr[g] = __ffma2_rn(m[g], w.nwi[g][k], __fmul2_rn(r[g], w.wr[g][k]));
+            cm[g] = __ffma2_rn(r[g], w.wi[g][k], __fmul2_rn(m[g], w.wr[g][k]));
+        }
+        meas_dfs<I + (1 << k), G>(cr, cm, w, sr, si);
+        meas_dfs_children<I, K - 1, G>(r, m, w, sr, si);
     }
 }
 
-template <int I>
-__device__ __forceinline__ void meas_dfs(float2 r, float2 m, const PairSteps &w,
-                                         float (&sr)[kBlockF], float (&si)[kBlockF]) {
-    sr[I] = r.x + r.y;
-    si[I] = m.x + m.y;
-    meas_dfs_children<I, dfs_child_bits(I)>(r, m, w, sr, si);
+// slot I of every pair folded into one scalar (the sum over the lane's 2G voxels), and the
+// transpose-reduce's first level (slot i += the xor-16 partner's slot i+16) done as soon as
+// both slots exist: the depth-first order makes slot i+16 before slot i (i > 0), and slot
+// 16 right after slot 0, so at most 17 slots per component are live at a time
+template <int I, int G>
+__device__ __forceinline__ void meas_dfs(const float2 (&r)[G], const float2 (&m)[G],
+                                         const PairSteps<G> &w, float (&sr)[kBlockF],
+                                         float (&si)[kBlockF]) {
+    float2 tr = r[0], tm = m[0];
+#pragma unroll
+    for (int g = 1; g < G; ++g) {
+        tr = __fadd2_rn(tr, r[g]);
+        tm = __fadd2_rn(tm, m[g]);
+    }
+    const float vr = tr.x + tr.y, vi = tm.x + tm.y;
+    if constexpr (I == 16) {
+        sr[0] += __shfl_xor_sync(0xffffffffu, vr, 16);
+        si[0] += __shfl_xor_sync(0xffffffffu, vi, 16);
+    } else if constexpr (I > 0 && I < 16) {
+        sr[I] = vr + __shfl_xor_sync(0xffffffffu, sr[I + 16], 16);
+        si[I] = vi + __shfl_xor_sync(0xffffffffu, si[I + 16], 16);
+    } else {
+        sr[I] = vr;
+        si[I] = vi;
+    }
+    meas_dfs_children<I, dfs_child_bits(I), G>(r, m, w, sr, si);
 }
 
 // Grid: (antennas / NW) x meas_splits; CTA (x, s) covers voxel range s, and with several
 // ranges writes its sums to the range's partial buffer (reduced in range order after).
-template <int MAXB, int NW>
-__global__ void __launch_bounds__(NW * 32) bp_bwd_meas3_kernel(const BwdParams bp) {
+// Every lane takes G voxel pairs (2G voxels) per pass: one transpose-reduce serves 64G.
+template <int MAXB, int NW, int G>
+__global__ void __launch_bounds__(NW * 32, 16 / NW) bp_bwd_meas3_kernel(const BwdParams bp) {
     const FwdParams &p = bp.f;
     __shared__ float4 vrec[kMeas2Chunk * 3];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -611,53 +640,63 @@ __global__ void __launch_bounds__(NW * 32) bp_bwd_meas3_kernel(const BwdParams b
         for (int q = threadIdx.x; q < nv * 3; q += NW * 32) vrec[q] = bp.vox_rec[v0 * 3 + q];
         __syncthreads();
         if (!active) continue;
-        for (int base = 0; base < nv; base += 64) {
-            PairSteps w;
-            float2 gr, gi;
-            unsigned long long ph[2], stp[2];
+        for (int base = 0; base < nv; base += 64 * G) {
+            PairSteps<G> w;
+            float2 gr[G], gi[G];
+            unsigned long long ph[G][2], stp[G][2];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int j = base + 32 * h + lane;
-                const bool vok = j < nv;
-                const float4 r0 = vrec[3 * (vok ? j : 0)];
-                const float4 r1 = vrec[3 * (vok ? j : 0) + 1];
-                const float4 r2 = vrec[3 * (vok ? j : 0) + 2];
-                const double d =
-                    range_fp64((double)r0.x, (double)r0.y, (double)r0.z, ar, mono, p.ti);
-                const float2 z = cis_fp64_phase(d * p.kd);  // conj of the forward step
-                float zr = z.x, zi = z.y;
+            for (int g = 0; g < G; ++g) {
 #pragma unroll
-                for (int k = 0; k < 5; ++k) {
-                    const float si = (lane & (1 << k)) ? -zi : zi;
-                    (h ? w.wr[k].y : w.wr[k].x) = zr;
-                    (h ? w.wi[k].y : w.wi[k].x) = si;
-                    (h ? w.nwi[k].y : w.nwi[k].x) = -si;
-                    const float nr = zr * zr - zi * zi;
-                    zi = 2.f * zr * zi;
-                    zr = nr;
+                for (int h = 0; h < 2; ++h) {
+                    const int j = base + 64 * g + 32 * h + lane;
+                    const bool vok = j < nv;
+                    const float4 r0 = vrec[3 * (vok ? j : 0)];
+                    const float4 r1 = vrec[3 * (vok ? j : 0) + 1];
+                    const float4 r2 = vrec[3 * (vok ? j : 0) + 2];
+                    const double d =
+                        range_fp64((double)r0.x, (double)r0.y, (double)r0.z, ar, mono, p.ti);
+                    const float2 z = cis_fp64_phase(d * p.kd);  // conj of the forward step
+                    float zr = z.x, zi = z.y;
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) {
+                        const float si = (lane & (1 << k)) ? -zi : zi;
+                        (h ? w.wr[g][k].y : w.wr[g][k].x) = zr;
+                        (h ? w.wi[g][k].y : w.wi[g][k].x) = si;
+                        (h ? w.nwi[g][k].y : w.nwi[g][k].x) = -si;
+                        const float nr = zr * zr - zi * zi;
+                        zi = 2.f * zr * zi;
+                        zr = nr;
+                    }
+                    const float ux = ar.virt[0] - r0.x, uy = ar.virt[1] - r0.y,
+                                uz = ar.virt[2] - r0.z;
+                    float Gr = fmaf(r2.z, uz, fmaf(r2.x, uy, fmaf(r1.z, ux, r1.x)));
+                    float Gi = fmaf(r2.w, uz, fmaf(r2.y, uy, fmaf(r1.w, ux, r1.y)));
+                    if (!vok) Gr = Gi = 0.f;
+                    (h ? gr[g].y : gr[g].x) = Gr;
+                    (h ? gi[g].y : gi[g].x) = Gi;
+                    ph[g][h] = turns_to_fixed(d * p.t0) +
+                               (unsigned long long)lane * turns_to_fixed(d * t1);
+                    stp[g][h] = turns_to_fixed(d * p.tblk);
                 }
-                const float ux = ar.virt[0] - r0.x, uy = ar.virt[1] - r0.y, uz = ar.virt[2] - r0.z;
-                float Gr = fmaf(r2.z, uz, fmaf(r2.x, uy, fmaf(r1.z, ux, r1.x)));
-                float Gi = fmaf(r2.w, uz, fmaf(r2.y, uy, fmaf(r1.w, ux, r1.y)));
-                if (!vok) Gr = Gi = 0.f;
-                (h ? gr.y : gr.x) = Gr;
-                (h ? gi.y : gi.x) = Gi;
-                ph[h] = turns_to_fixed(d * p.t0) + (unsigned long long)lane * turns_to_fixed(d * t1);
-                stp[h] = turns_to_fixed(d * p.tblk);
             }
 #pragma unroll 1
             for (int b = 0; b < nblk; ++b) {
-                float2 ac, as;
-                fixed_cis(ph[0], ac.x, as.x);
-                fixed_cis(ph[1], ac.y, as.y);
-                ph[0] += stp[0];
-                ph[1] += stp[1];
+                float2 r[G], m[G];
+#pragma unroll
+                for (int g = 0; g < G; ++g) {
+                    float2 ac, as;
+                    fixed_cis(ph[g][0], ac.x, as.x);
+                    fixed_cis(ph[g][1], ac.y, as.y);
+                    ph[g][0] += stp[g][0];
+                    ph[g][1] += stp[g][1];
+                    // slot 0: G * anchor (both halves)
+                    r[g] = __ffma2_rn(gr[g], ac, __fmul2_rn(gi[g], make_float2(-as.x, -as.y)));
+                    m[g] = __ffma2_rn(gr[g], as, __fmul2_rn(gi[g], ac));
+                }
                 float sr[kBlockF], si[kBlockF];
-                // slot 0: G * anchor (both halves), then the depth-first slot tree
-                meas_dfs<0>(__ffma2_rn(gr, ac, __fmul2_rn(gi, make_float2(-as.x, -as.y))),
-                            __ffma2_rn(gr, as, __fmul2_rn(gi, ac)), w, sr, si);
-                warp_transpose_reduce32(sr);
-                warp_transpose_reduce32(si);
+                meas_dfs<0, G>(r, m, w, sr, si);  // the depth-first slot tree, level 0 folded
+                warp_transpose_reduce32(sr, 1);
+                warp_transpose_reduce32(si, 1);
 #pragma unroll
                 for (int bb = 0; bb < MAXB; ++bb)
                     if (bb == b) {
@@ -744,6 +783,9 @@ cudaError_t launch_bwd_pos_reduce(const BwdParams &bp, cudaStream_t stream) {
 }
 
 constexpr int kMeas3Warps = 4;  // 4 warps per CTA: three CTAs per SM at ~150 registers
+// voxel pairs per lane and pass: 2 halves the transposes per update but needs ~254
+// registers (two CTAs, 8 warps per SM) and measured no faster than 1 (38.6 vs 38.3 ms)
+constexpr int kMeasPairs = 1;
 
 int bwd_meas_splits(int num_ant, int fp, int64_t nvox) {
     const int nblk = fp / kBlockF;
@@ -751,8 +793,8 @@ int bwd_meas_splits(int num_ant, int fp, int64_t nvox) {
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const void *fn = nblk <= 4 ? reinterpret_cast<const void *>(&bp_bwd_meas3_kernel<4, kMeas3Warps>)
-                               : reinterpret_cast<const void *>(&bp_bwd_meas3_kernel<8, kMeas3Warps>);
+    const void *fn = nblk <= 4 ? reinterpret_cast<const void *>(&bp_bwd_meas3_kernel<4, kMeas3Warps, kMeasPairs>)
+                               : reinterpret_cast<const void *>(&bp_bwd_meas3_kernel<8, kMeas3Warps, kMeasPairs>);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMeas3Warps * 32, 0) !=
             cudaSuccess ||
         per_sm < 1)
@@ -780,9 +822,9 @@ cudaError_t launch_bwd_meas(const BwdParams &bp, cudaStream_t stream) {
     const dim3 grid3((bp.num_ant_real + kMeas3Warps - 1) / kMeas3Warps, bp.meas_splits);
     if (nblk <= 8) {
         if (nblk <= 4)
-            bp_bwd_meas3_kernel<4, kMeas3Warps><<<grid3, kMeas3Warps * 32, 0, stream>>>(bp);
+            bp_bwd_meas3_kernel<4, kMeas3Warps, kMeasPairs><<<grid3, kMeas3Warps * 32, 0, stream>>>(bp);
         else
-            bp_bwd_meas3_kernel<8, kMeas3Warps><<<grid3, kMeas3Warps * 32, 0, stream>>>(bp);
+            bp_bwd_meas3_kernel<8, kMeas3Warps, kMeasPairs><<<grid3, kMeas3Warps * 32, 0, stream>>>(bp);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess || bp.meas_splits <= 1) return e;
         const int64_t n = (int64_t)bp.num_ant_real * bp.num_samples;
