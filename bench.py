@@ -415,6 +415,25 @@ def ours_arm(args):
                "path": "pinned host -> ops.backproject + image_max_abs (+ all-reduce) + "
                        "surface_normals_from_max (C ABI) -> pinned host image + unit normals"}
 
+    # the reference-facing call a mmNorm user makes (image_processor.py:383-396's image and
+    # normals in one call, numpy in and out), on rank 0 of a single-GPU run
+    e2e_dropin = None
+    if rank == 0 and world == 1 and not args.no_e2e:
+        from mmnorm_b200 import pipeline
+        radar = sc.meas[:, :, None]
+        args_d = (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs.astype(np.float64), radar,
+                  np.zeros((1, 3)), sc.slope, sc.wavelength, sc.slope * (F - 1), F)
+        pipeline.surface_normals(*args_d, use_4_rx=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pipeline.surface_normals(*args_d, use_4_rx=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        e2e_dropin = {"value": updates / dt / 1e9, "unit": UNIT, "seconds": dt,
+                      "path": "pipeline.surface_normals (image_cuda + normal_estimates_cuda "
+                              "semantics): numpy inputs -> complex64 image, float64 unit "
+                              "normals with NaN, phase centres; wall clock, one call"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -503,6 +522,7 @@ def ours_arm(args):
                          "fp32_lane_bound_8_ops": lane_bounds(updates / kern_avg_s, 128 / 8)},
             "clocks": clk,
             "e2e": e2e,
+            "e2e_dropin": e2e_dropin,
             "gpu_launches": launches_per_step * args.steps,
             "cpu_baseline": cpu,
             "numpy_baseline": numpy_cpu,
