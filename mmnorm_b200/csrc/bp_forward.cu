@@ -407,7 +407,10 @@ __global__ void __launch_bounds__(NT) bp_fwd_persistent(const BatchParams bp) {
         __syncthreads();
         if (item >= bp.num_items) break;
         const int4 w = bp.items[item];
-        if (!fwd_item<T, NT, FORM, ANCHOR, true>(bp.objs[w.x], w.y, w.z, smem, gchunk)) break;
+        // the item's object parameters as a local copy: read once, then kept in registers
+        // (a reference into global memory would be re-read inside the loops)
+        const FwdParams obj = bp.objs[w.x];
+        if (!fwd_item<T, NT, FORM, ANCHOR, true>(obj, w.y, w.z, smem, gchunk)) break;
     }
 }
 
