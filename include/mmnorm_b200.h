@@ -344,6 +344,18 @@ int mmn_cuda_sn_est(float *normals_x, float *normals_y, float *normals_z,
 int mmn_fp32_peak_probe(int blocks, int iters, float *out, cudaStream_t stream);
 
 /*
+ * Bounded-wait check (no counterpart in the reference, whose kernels have no waits): one
+ * warp waits on an mbarrier with the same bounded wait the copy pipelines use (which give up
+ * after one second), here giving up after `limit_us` microseconds (at most 10 s, else
+ * MMN_ERR_INVALID_ARGUMENT).  With `arrive` != 0 the phase is completed first and the wait
+ * succeeds; with `arrive` == 0 nothing completes it, the wait runs out and the kernel
+ * records MMN_ERR_TIMEOUT in the status word at the start of `workspace` (read and clear it
+ * with mmn_read_status) and returns.  Nothing faults and the context stays usable.
+ */
+int mmn_wait_timeout_probe(uint32_t limit_us, int arrive, void *workspace,
+                           cudaStream_t stream);
+
+/*
  * Status word that kernels set when a bounded wait gives up (MMN_ERR_TIMEOUT) -- kept in
  * the first bytes of every workspace.  Synchronises `stream`, copies the word to the
  * host, and clears it.  Returns MMN_OK or the CUDA error; *status receives the word.

@@ -121,6 +121,7 @@ SIGNATURES = [
     ("mmn_cuda_sn_est", _I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _F,
                              _F, _F, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _SZ, _P]),
     ("mmn_fp32_peak_probe", _I, [_I, _I, _P, _P]),
+    ("mmn_wait_timeout_probe", _I, [ctypes.c_uint32, _I, _P, _P]),
     ("mmn_batch_create", _I, [_PROB, _I32, _I32, _P, _P, _I32, ctypes.POINTER(_P),
                               ctypes.POINTER(_SZ)]),
     ("mmn_batch_upload", _I, [_P, _P, _SZ, _P]),

@@ -177,14 +177,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait on an mbarrier phase.  Each try_wait suspends for a hardware-defined
-// interval; after kMaxPolls unsuccessful polls (well beyond any legitimate copy) the
-// wait gives up, records MMN_ERR_TIMEOUT and returns false.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on an mbarrier phase.  An unsatisfied try_wait suspends the thread for a
+// hardware-defined interval (about 4 us on B200), so the bound is set in time: after
+// kWaitLimitNs of %globaltimer (a second, far beyond any legitimate copy) the wait gives up,
+// records MMN_ERR_TIMEOUT and returns false.  kMaxPolls caps the polls as well, in case the
+// timer does not advance.  The first poll reads no timer, so a completed phase costs one
+// try_wait.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
 constexpr uint32_t kMaxPolls = 1u << 24;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
-                                                  int32_t *status) {
-    for (uint32_t i = 0; i < kMaxPolls; ++i)
+                                                  int32_t *status,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < kMaxPolls; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) break;
+    }
     set_status(status, MMN_ERR_TIMEOUT);
     return false;
 }
