@@ -574,13 +574,25 @@ def time_adjoint(dev):
                                                    pos_offsets=pos, want_pos=False))
     bwd_p = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
                                                    pos_offsets=pos, want_meas=False))
-    # a loss on the image only (no vote term): one Horner chain in the position pass
+    # a loss on the image only (no vote term): the position pass skips the vote terms
     bwd_i = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, None,
                                                    pos_offsets=pos))
+    # the position pass's Horner form (two FP32 chains over all samples), for comparison
+    ops.set_position_pass("horner")
+    try:
+        hor = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
+                                                     pos_offsets=pos))
+        hor_p = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
+                                                       pos_offsets=pos, want_meas=False))
+    finally:
+        ops.set_position_pass("interp")
     return {"workload": sc.name + " (64^3 voxels @3 mm, 64x64 antennas @3 mm, 128 freqs)",
             "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
             "backward_meas_ms": bwd_m, "backward_pos_ms": bwd_p,
-            "backward_image_loss_ms": bwd_i, "backward_image_loss_over_forward": bwd_i / fwd}
+            "position_pass": "interpolation (8-cell kernel, 2x oversampled per-antenna grid)",
+            "backward_image_loss_ms": bwd_i, "backward_image_loss_over_forward": bwd_i / fwd,
+            "horner_position_pass": {"backward_ms": hor, "backward_pos_ms": hor_p,
+                                     "backward_over_forward": hor / fwd}}
 
 
 def time_batched(dev, replays=3):

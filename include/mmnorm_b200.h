@@ -113,6 +113,23 @@ int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
                              void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /*
+ * How the backward evaluates the two per-(voxel, antenna) sample sums the position
+ * gradient needs (no reference counterpart).  MMN_POS_INTERP (the default): interpolation
+ * with an 8-cell exponential-of-semicircle kernel from each antenna's spectrum on a 2x
+ * oversampled grid (a type-2 non-uniform FFT; ~1e-7 relative, the FP32 chains' level),
+ * used when F <= ~1500; MMN_POS_HORNER: two FP32 Horner chains over all F samples, as the
+ * forward evaluates its sum.  Process-wide; the measurement gradient is the same in both.
+ */
+#define MMN_POS_INTERP 0
+#define MMN_POS_HORNER 1
+int mmn_set_position_pass(int32_t form);
+/* Launch shapes of the interpolation form (voxels per thread, threads, stage size) for the
+ * autotuner; process-wide, like mmn_set_variant. */
+int mmn_num_position_variants(void);
+const char *mmn_position_variant_name(int32_t idx); /* NULL for a bad index */
+int mmn_set_position_variant(int32_t idx);
+
+/*
  * Batched persistent launch (no counterpart in the reference, which images one object per
  * call; mmwave_reconstruction.sh:61-69 loops over objects in the shell).  Many objects --
  * each its own voxel grid, aperture, sample count and radar constants -- run in ONE

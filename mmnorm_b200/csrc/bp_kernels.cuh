@@ -79,7 +79,16 @@ struct BwdParams {
     int32_t meas_splits;       // voxel ranges of the measurement pass (1: no partial sums)
     float2 *meas_partial;      // [meas_splits, num_ant_real, num_samples] if meas_splits > 1
     int64_t vox_per_split;     // voxels per measurement-pass range (a multiple of 512)
+    int32_t nu_n;              // interpolation-form position pass: grid cells N = 2F
+    int32_t pad_nu;
+    double nu_u;               // slope / c: turns per sample per metre of range
+    double nu_k0c;             // 2pi (1/lambda + J0 slope/c), J0 = F/2: anchor phase per metre
 };
+
+// Interpolation-form position pass (bp_pos_nufft.cu): kernel width in grid cells, and the
+// length of one antenna's staged grid row (N + W - 1 cells, so that no tap run wraps).
+constexpr int kNuW = 8;
+__host__ __device__ constexpr int nufft_row(int n) { return n + kNuW - 1; }
 
 cudaError_t launch_bwd_stage(const float *meas, int A, int F, int Fp, double k0, double kd,
                              int layout, void *dst, cudaStream_t stream);
@@ -92,6 +101,16 @@ int bwd_meas_splits(int num_ant, int fp, int64_t nvox);
 const void *bwd_pos_kernel_ptr(int variant, int *threads, int *voxels_per_thread);
 // position pass for losses without a vote term (launch_bwd_pos with variant -1)
 const void *bwd_pos_img_kernel_ptr(int *threads, int *voxels_per_thread);
+// interpolation-form position pass (vote: the loss has a vote term) and its per-antenna
+// grids: tables (tw [N] double2, 16-byte aligned; sc [F] doubles) and rows
+// [A][nufft_row(N)] float4
+const void *bwd_pos_nufft_kernel_ptr(int variant, bool vote, int *threads, int *voxels_per_thread,
+                                     int *stage_cap_bytes);
+int bwd_pos_nufft_num_variants();
+const char *bwd_pos_nufft_variant_name(int variant);  // null for a bad index
+cudaError_t launch_nufft_grid(const float *meas, int A, int F, int N, int J0, double k0,
+                              double kd, double *sc, double2 *tw, float4 *rows,
+                              cudaStream_t stream);
 
 // ---------------------------------------------------------- interpolated mode
 struct InterpParams {

@@ -584,27 +584,44 @@ int mmn_read_status(void *workspace, int32_t *status, cudaStream_t stream) {
 namespace {
 
 std::atomic<int> g_bwd_variant{0};
+std::atomic<int> g_pos_form{MMN_POS_INTERP};
+std::atomic<int> g_pos_variant{0};
 
 struct BwdPlan {
     int fp, ant_per_stage, tiles, splits, ant_per_split, threads, vpt;
     size_t smem;
-    size_t off_ant, off_meas, off_vox, off_pos, off_mpart, total;
+    size_t off_ant, off_meas, off_vox, off_pos, off_mpart, off_nutab, total;
     int meas_splits;
     int64_t vox_per_split;
     const void *fn;
+    bool nufft;  // position pass in interpolation form
+    int nu_n, row;
 };
 
-// image_only: the loss has no vote term (grad_vote NULL), so the position pass needs one
-// Horner chain per voxel-antenna and runs the voxel-pair kernel.
-int plan_backward(const mmn_problem *p, bool image_only, BwdPlan *pl) {
+// image_only: the loss has no vote term (grad_vote NULL): the Horner form needs one chain
+// per voxel-antenna and runs the voxel-pair kernel; the interpolation form skips the vote
+// terms.  form: MMN_POS_INTERP (used when one staged grid row fits a shared-memory stage,
+// i.e. F up to about 1500) or MMN_POS_HORNER.
+int plan_backward(const mmn_problem *p, bool image_only, int form, BwdPlan *pl) {
     const int A = p->num_antennas;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
-    pl->fn = image_only ? bwd_pos_img_kernel_ptr(&pl->threads, &pl->vpt)
-                        : bwd_pos_kernel_ptr(g_bwd_variant.load(), &pl->threads, &pl->vpt);
     pl->fp = (p->num_samples + kBlockF - 1) / kBlockF * kBlockF;
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
-    const int rec = (int)sizeof(AntRec) + pl->fp * 16;
-    pl->ant_per_stage = std::max(1, std::min(16, kMaxStageBytes / rec));
+    pl->nu_n = 2 * p->num_samples;
+    pl->nufft = form == MMN_POS_INTERP &&
+                (int)sizeof(AntRec) + nufft_row(pl->nu_n) * 16 <= kMaxStageBytes;
+    int cap = kMaxStageBytes;
+    if (pl->nufft) {
+        pl->fn = bwd_pos_nufft_kernel_ptr(g_pos_variant.load(), !image_only, &pl->threads,
+                                          &pl->vpt, &cap);
+        pl->row = nufft_row(pl->nu_n);
+    } else {
+        pl->fn = image_only ? bwd_pos_img_kernel_ptr(&pl->threads, &pl->vpt)
+                            : bwd_pos_kernel_ptr(g_bwd_variant.load(), &pl->threads, &pl->vpt);
+        pl->row = pl->fp;
+    }
+    const int rec = (int)sizeof(AntRec) + pl->row * 16;
+    pl->ant_per_stage = std::max(1, std::min(16, cap / rec));
     pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec +
                (size_t)(pl->threads / 32) * pl->ant_per_stage * 3 * sizeof(float);
     const int64_t per_tile = (int64_t)pl->threads * pl->vpt;
@@ -642,7 +659,11 @@ int plan_backward(const mmn_problem *p, bool image_only, BwdPlan *pl) {
     pl->off_ant = off;
     off = align_up(off + (size_t)A * sizeof(AntRec));
     pl->off_meas = off;
-    off = align_up(off + (size_t)A * pl->fp * 16);
+    off = align_up(off + (size_t)A * pl->row * 16);
+    pl->off_nutab = off;  // interpolation form: twiddles [N] double2, then 1/phihat [F] doubles
+    if (pl->nufft)
+        off = align_up(off + (size_t)p->num_samples * sizeof(double) +
+                       (size_t)pl->nu_n * sizeof(double2));
     pl->off_vox = off;
     off = align_up(off + (size_t)nvox * 3 * sizeof(float4));
     pl->off_pos = off;
@@ -662,10 +683,32 @@ int plan_backward(const mmn_problem *p, bool image_only, BwdPlan *pl) {
 
 extern "C" size_t mmn_backward_workspace_bytes(const mmn_problem *p) {
     if (check_problem(p, MMN_MODE_MIXED) != MMN_OK) return 0;
-    BwdPlan pl, pl_img;
-    if (plan_backward(p, false, &pl) != MMN_OK) return 0;
-    if (plan_backward(p, true, &pl_img) != MMN_OK) return 0;
-    return std::max(pl.total, pl_img.total);
+    size_t total = 0;
+    for (int form = 0; form < 2; ++form) {
+        BwdPlan pl, pl_img;
+        if (plan_backward(p, false, form, &pl) != MMN_OK) return 0;
+        if (plan_backward(p, true, form, &pl_img) != MMN_OK) return 0;
+        total = std::max(total, std::max(pl.total, pl_img.total));
+    }
+    return total;
+}
+
+extern "C" int mmn_set_position_pass(int32_t form) {
+    if (form != MMN_POS_INTERP && form != MMN_POS_HORNER) return MMN_ERR_INVALID_ARGUMENT;
+    g_pos_form.store(form);
+    return MMN_OK;
+}
+
+extern "C" int mmn_num_position_variants(void) { return bwd_pos_nufft_num_variants(); }
+
+extern "C" const char *mmn_position_variant_name(int32_t idx) {
+    return bwd_pos_nufft_variant_name(idx);
+}
+
+extern "C" int mmn_set_position_variant(int32_t idx) {
+    if (idx < 0 || idx >= bwd_pos_nufft_num_variants()) return MMN_ERR_INVALID_ARGUMENT;
+    g_pos_variant.store(idx);
+    return MMN_OK;
 }
 
 extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
@@ -683,7 +726,7 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     if (A == 0) return MMN_OK;
     const bool image_only = grad_vote == nullptr;
     BwdPlan pl;
-    rc = plan_backward(p, image_only, &pl);
+    rc = plan_backward(p, image_only, g_pos_form.load(), &pl);
     if (rc != MMN_OK) return rc;
     if (workspace_bytes < pl.total) return MMN_ERR_WORKSPACE;
     unsigned char *ws = static_cast<unsigned char *>(workspace);
@@ -732,7 +775,26 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     bp.meas_splits = pl.meas_splits;
     bp.meas_partial = reinterpret_cast<float2 *>(ws + pl.off_mpart);
     bp.vox_per_split = pl.vox_per_split;
-    if (grad_pos) {
+    if (grad_pos && pl.nufft) {
+        const int J0 = F / 2;
+        double2 *tw = reinterpret_cast<double2 *>(ws + pl.off_nutab);  // 256-aligned
+        double *sc = reinterpret_cast<double *>(tw + pl.nu_n);
+        if (launch_nufft_grid(p->meas, A, F, pl.nu_n, J0, f.k0, f.kd, sc, tw,
+                              reinterpret_cast<float4 *>(ws + pl.off_meas), stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+        BwdParams bq = bp;
+        bq.f.fp = pl.row;
+        bq.nu_n = pl.nu_n;
+        bq.nu_u = p->slope / kC;
+        bq.nu_k0c = 2.0 * kPi * (1.0 / p->wavelength + (double)J0 * p->slope / kC);
+        if (pl.smem > 48 * 1024)
+            cudaFuncSetAttribute(pl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+        void *args[] = {&bq};
+        if (cudaLaunchKernel(pl.fn, dim3(pl.tiles * pl.splits), dim3(pl.threads), args, pl.smem,
+                             stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+        if (launch_bwd_pos_reduce(bp, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    } else if (grad_pos) {
         if (launch_bwd_stage(p->meas, A, F, pl.fp, f.k0, f.kd, image_only ? 1 : 0,
                              ws + pl.off_meas, stream) != cudaSuccess)
             return MMN_ERR_CUDA;

@@ -217,6 +217,27 @@ def set_variant(mode, index):
     _lib.check(_lib.load().mmn_set_variant(_lib.MODES[mode], int(index)), "mmn_set_variant")
 
 
+POSITION_PASSES = {"interp": 0, "horner": 1}
+
+
+def set_position_pass(form):
+    """How the backward evaluates the position gradient's per-(voxel, antenna) sample sums:
+    "interp" (default; interpolation from a 2x oversampled per-antenna spectrum, F <= ~1500)
+    or "horner" (two FP32 Horner chains over all samples).  Process-wide."""
+    _lib.check(_lib.load().mmn_set_position_pass(POSITION_PASSES[form]), "mmn_set_position_pass")
+
+
+def position_variants():
+    """Launch shapes of the interpolation-form position pass, by index."""
+    lib = _lib.load()
+    return [lib.mmn_position_variant_name(i).decode()
+            for i in range(lib.mmn_num_position_variants())]
+
+
+def set_position_variant(index):
+    _lib.check(_lib.load().mmn_set_position_variant(int(index)), "mmn_set_position_variant")
+
+
 def backproject_backward(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength,
                          slope, grad_image, grad_vote, *, is_ti_radar=False, pos_offsets=None,
                          want_meas=True, want_pos=True):

@@ -81,7 +81,15 @@ def _problem(dev, n_ap=16, n_vox=16, nf=128, seed=0):
     return sc, t, rng, torch.as_tensor(nt.T.copy(), device=dev)
 
 
-def test_adjoint_matches_oracle(cuda_dev, oracle):
+@pytest.fixture(params=["interp", "horner"])
+def pos_form(request):
+    from mmnorm_b200 import ops
+    ops.set_position_pass(request.param)
+    yield request.param
+    ops.set_position_pass("interp")
+
+
+def test_adjoint_matches_oracle(cuda_dev, oracle, pos_form):
     import torch
     from mmnorm_b200 import ops
     sc = scenes.sphere_scene(seed=41, n_ap=6, nf=40, n_vox=5, n_pts=10)
@@ -102,7 +110,7 @@ def test_adjoint_matches_oracle(cuda_dev, oracle):
     assert oracle.rel_l2(gp.cpu().numpy(), gp_o) < 2e-4
 
 
-def test_gradients_vs_dense_fp64_and_finite_differences(cuda_dev):
+def test_gradients_vs_dense_fp64_and_finite_differences(cuda_dev, pos_form):
     import torch
     from mmnorm_b200 import ops
     sc, t, rng, n_true = _problem(cuda_dev)
@@ -188,10 +196,10 @@ def test_adjoint_dot_product_identity(cuda_dev):
     assert abs(float(lhs - rhs)) <= 2e-5 * abs(float(lhs))
 
 
-def test_image_only_position_gradient(cuda_dev, oracle):
-    """Without a vote term the position pass runs one Horner chain per voxel-antenna (voxel
-    pairs in the FFMA2 halves); it must agree with the oracle's adjoint and with the
-    two-chain kernel given an all-zero vote gradient."""
+def test_image_only_position_gradient(cuda_dev, oracle, pos_form):
+    """Without a vote term the position pass skips the vote terms (Horner form: one chain
+    per voxel-antenna, voxel pairs in the FFMA2 halves); it must agree with the oracle's
+    adjoint and with the full kernel given an all-zero vote gradient."""
     import torch
     from mmnorm_b200 import ops
     sc = scenes.sphere_scene(seed=44, n_ap=10, nf=72, n_vox=9, n_pts=20)
@@ -221,3 +229,74 @@ def test_image_only_position_gradient(cuda_dev, oracle):
     (I.reshape(-1).conj() * _t(gI, cuda_dev)).real.sum().backward()
     assert oracle.rel_l2(pos.grad.cpu().numpy().astype(np.float64),
                          gp1.cpu().numpy().astype(np.float64)) < 1e-6
+
+
+@pytest.mark.parametrize("nf", [1, 3, 40, 129])
+def test_interpolation_form_matches_horner_form(cuda_dev, oracle, nf):
+    """The position pass's two forms on the same problem, over sample counts down to one
+    (grid of 2 cells, narrower than the 8-cell kernel: taps wrap around the grid several
+    times) and odd counts (J0 = F/2 rounds down); both against the oracle."""
+    import torch
+    from mmnorm_b200 import ops
+    sc = scenes.sphere_scene(seed=45 + nf, n_ap=7, nf=max(nf, 2), n_vox=7, n_pts=12)
+    meas = np.ascontiguousarray(sc.meas[:, :nf])
+    rng = np.random.default_rng(45)
+    rxo = np.array([[0.0, -0.004, 0.001]], np.float32)
+    V = sc.num_voxels
+    gI = (rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64)
+    gW = (rng.standard_normal((3, V)) + 1j * rng.standard_normal((3, V))).astype(np.complex64)
+    args = [_t(a, cuda_dev) for a in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs, rxo,
+                                      meas)]
+    out = {}
+    try:
+        for form in ("interp", "horner"):
+            ops.set_position_pass(form)
+            out[form] = ops.backproject_backward(*args, sc.wavelength, sc.slope,
+                                                 _t(gI, cuda_dev), _t(gW, cuda_dev),
+                                                 want_meas=False)[1]
+    finally:
+        ops.set_position_pass("interp")
+    torch.cuda.synchronize()
+    _, gp_o = oracle.full_backward(sc.voxel_centres(), sc.antenna_locs, rxo, meas,
+                                   sc.wavelength, sc.slope, gI.astype(np.complex128),
+                                   gW.T.astype(np.complex128))
+    a, b = (out[f].cpu().numpy().astype(np.float64) for f in ("interp", "horner"))
+    assert oracle.rel_l2(a, gp_o) < 2e-4 and oracle.rel_l2(b, gp_o) < 2e-4
+    assert oracle.rel_l2(a, b) < 2e-5
+
+
+def test_position_variants_agree(cuda_dev, oracle):
+    """Every launch shape of the interpolation form gives the oracle's position gradient
+    (voxel-to-thread mapping and summation order differ, the values only by rounding)."""
+    import torch
+    from mmnorm_b200 import ops
+    sc = scenes.sphere_scene(seed=47, n_ap=12, nf=48, n_vox=11, n_pts=16)
+    rng = np.random.default_rng(47)
+    rxo = np.array([[0.0, -0.004, 0.001]], np.float32)
+    V = sc.num_voxels
+    gI = (rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64)
+    gW = (rng.standard_normal((3, V)) + 1j * rng.standard_normal((3, V))).astype(np.complex64)
+    args = [_t(a, cuda_dev) for a in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs, rxo,
+                                      sc.meas)]
+    _, gp_o = oracle.full_backward(sc.voxel_centres(), sc.antenna_locs, rxo, sc.meas,
+                                   sc.wavelength, sc.slope, gI.astype(np.complex128),
+                                   gW.T.astype(np.complex128))
+    names = ops.position_variants()
+    assert len(names) >= 2
+    outs = []
+    try:
+        for i in range(len(names)):
+            ops.set_position_variant(i)
+            for g in (_t(gW, cuda_dev), None):
+                gp = ops.backproject_backward(*args, sc.wavelength, sc.slope, _t(gI, cuda_dev),
+                                              g, want_meas=False)[1]
+                outs.append((i, g is None, gp.cpu().numpy().astype(np.float64)))
+    finally:
+        ops.set_position_variant(0)
+    _, gp_img = oracle.full_backward(sc.voxel_centres(), sc.antenna_locs, rxo, sc.meas,
+                                     sc.wavelength, sc.slope, gI.astype(np.complex128),
+                                     np.zeros((V, 3), np.complex128))
+    for i, img, gp in outs:
+        assert oracle.rel_l2(gp, gp_img if img else gp_o) < 2e-4, (names[i], img)
+    with pytest.raises(Exception):
+        ops.set_position_variant(len(names))
