@@ -10,9 +10,9 @@
 //   M(u) ~= sum_k phi(N u - k) G_k,   G_k = sum_j' (m / phihat(j'/N)) e^{-2pi i j' k / N},
 // with phi the exponential-of-semicircle kernel exp(beta (sqrt(1 - (2z/W)^2) - 1)),
 // W = 8 cells, beta = 2.3 W, and phihat its Fourier transform.  Per (voxel, antenna) that
-// is eight taps -- each a degree-8 polynomial in the fractional cell offset for its weight
-// (es_taps.cuh, FP32 Horner with constant-bank coefficients), one 16-byte shared load of
-// (G'.re, G.re, G'.im, G.im) and two FFMA2 -- in place of two F-step Horner chains.
+// is eight taps -- weights from degree-8 polynomials in the fractional cell offset
+// (es_taps.cuh; mirror taps share one even and one odd part), one 16-byte shared load of
+// (G'.re, G.re, G'.im, G.im) and two FFMA2 each -- in place of two F-step Horner chains.
 // Accuracy ~1e-7 relative (the FP32 Horner chains' level).
 //
 // Kernels: nufft_tables_kernel (1/phihat by midpoint quadrature in FP64, twiddles),
@@ -39,6 +39,82 @@ __device__ __forceinline__ double es_kernel(double z) {
 }
 
 }  // namespace
+
+// Per (voxel, antenna) geometry of the interpolation form.
+//   d      round-trip range in FP64.  Each leg's square root starts from an FP32 rsqrt of the
+//          FP32 difference vector and takes one FP64 Newton step (relative error ~1e-13, far
+//          below what the phase needs), which avoids the IEEE FP64 square root's slow path.
+//   e3     -(unit(v - tx) + unit(v - rx)) in FP32 (the derivative of d with respect to an
+//          antenna offset; a direction needs no more).
+//   ix, s  grid cell and fractional offset of N * (u mod 1), u = d slope/c, reduced with the
+//          1.5*2^52 rounding constant (no conversion instructions); clamped so that a NaN or a
+//          fraction that rounds up to 1 still reads inside the row.
+//   w[8]   tap weights (es_taps.cuh): P_i(t) and P_i(-t) from one even and one odd part.
+struct NuPair {
+    double d;
+    float e3[3];
+    int ix;
+    float w[kNuW];
+};
+
+__device__ __forceinline__ void nufft_pair(double vxd, double vyd, double vzd, float vx, float vy,
+                                           float vz, const AntRec &ar, const float (&txf)[3],
+                                           const float (&rxf)[3], bool mono, double ti, double uq,
+                                           int n, NuPair &o) {
+    const float ax = vx - txf[0], ay = vy - txf[1], az = vz - txf[2];
+    const float rf = rsqrtf(fmaf(ax, ax, fmaf(ay, ay, az * az)));
+    const double dx = vxd - ar.tx[0], dy = vyd - ar.tx[1], dz = vzd - ar.tx[2];
+    const double D = fma(dx, dx, fma(dy, dy, dz * dz));
+    const double r = (double)rf;
+    double f = D * r;
+    f = fma(fma(-f, f, D), 0.5 * r, f);
+    double b = f;
+    float bx = ax, by = ay, bz = az, rb = rf;
+    if (!mono) {
+        bx = vx - rxf[0];
+        by = vy - rxf[1];
+        bz = vz - rxf[2];
+        rb = rsqrtf(fmaf(bx, bx, fmaf(by, by, bz * bz)));
+        const double ex = vxd - ar.rx[0], ey = vyd - ar.rx[1], ez = vzd - ar.rx[2];
+        const double B = fma(ex, ex, fma(ey, ey, ez * ez));
+        const double rr = (double)rb;
+        b = B * rr;
+        b = fma(fma(-b, b, B), 0.5 * rr, b);
+    }
+    o.d = f + b + ti;
+    o.e3[0] = -fmaf(ax, rf, bx * rb);
+    o.e3[1] = -fmaf(ay, rf, by * rb);
+    o.e3[2] = -fmaf(az, rf, bz * rb);
+
+    const double kRound = 6755399441055744.0;  // 1.5 * 2^52
+    const double u = o.d * uq;
+    double uf = u - ((u + kRound) - kRound);  // [-1/2, 1/2]
+    uf = uf < 0.0 ? uf + 1.0 : uf;            // [0, 1]
+    const double x = uf * (double)n;
+    const double xt = x + kRound;
+    int ix = __double2loint(xt);
+    double fr = x - (xt - kRound);             // [-1/2, 1/2]
+    ix = fr < 0.0 ? ix - 1 : ix;
+    fr = fr < 0.0 ? fr + 1.0 : fr;
+    float sfr = (float)fr;
+    const bool lo = !(ix >= 0), hi = ix >= n;
+    ix = lo ? 0 : (hi ? n - 1 : ix);
+    sfr = lo ? 0.f : (hi ? 1.f : sfr);
+    o.ix = ix;
+
+    const float t = sfr - 0.5f, t2 = t * t;
+#pragma unroll
+    for (int i = 0; i < kNuW / 2; ++i) {
+        float e = kEsEven[i][kEsEvenTerms - 1];
+#pragma unroll
+        for (int q = kEsEvenTerms - 2; q >= 0; --q) e = fmaf(e, t2, kEsEven[i][q]);
+        float od = kEsOdd[i][kEsOddTerms - 1];
+#pragma unroll
+        for (int q = kEsOddTerms - 2; q >= 0; --q) od = fmaf(od, t2, kEsOdd[i][q]);
+        o.w[i] = fmaf(t, od, e);
+        o.w[kNuW - 1 - i] = fmaf(-t, od, e);
+    }
+}
 
 // sc[j] = 1 / phihat((j - J0) / N) for j < F (one warp per j), tw[k] = e^{-2pi i k/N}.
 __global__ void nufft_tables_kernel(int F, int N, int J0, double *__restrict__ sc,
@@ -168,43 +244,17 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_nufft_kernel(const BwdParams bp
             float g3[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int k = 0; k < T; ++k) {
-                const double dx = vxd[k] - ar.tx[0], dy = vyd[k] - ar.tx[1],
-                             dz = vzd[k] - ar.tx[2];
-                const double f = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
-                double b = f;
-                if (!mono) {
-                    const double bx = vxd[k] - ar.rx[0], by = vyd[k] - ar.rx[1],
-                                 bz = vzd[k] - ar.rx[2];
-                    b = sqrt(fma(bx, bx, fma(by, by, bz * bz)));
-                }
-                const double d = f + b + p.ti;
-                // -(e_tx + e_rx): derivative of d with respect to the antenna offset
-                const float rf = 1.f / (float)f, rb = mono ? rf : 1.f / (float)b;
-                float e3[3];
-                e3[0] = -fmaf(vx[k] - txf[0], rf, (vx[k] - rxf[0]) * rb);
-                e3[1] = -fmaf(vy[k] - txf[1], rf, (vy[k] - rxf[1]) * rb);
-                e3[2] = -fmaf(vz[k] - txf[2], rf, (vz[k] - rxf[2]) * rb);
-
-                // grid position of u = d slope/c (mod 1) in cells; clamped so that a NaN or a
-                // fraction that rounds up to 1 still reads inside the row
-                const double u = d * uq;
-                const double xg = (u - floor(u)) * (double)n;
-                int ix = (int)xg;
-                float sfr = (float)(xg - (double)ix);
-                if (!(ix >= 0 && ix < n)) {
-                    ix = ix >= n ? n - 1 : 0;
-                    sfr = ix == 0 ? 0.f : 1.f;
-                }
-                // taps: weight_i(s) polynomials (es_taps.cuh), Horner in FP32
+                NuPair g;
+                nufft_pair(vxd[k], vyd[k], vzd[k], vx[k], vy[k], vz[k], ar, txf, rxf, mono, p.ti,
+                           uq, n, g);
+                const double d = g.d;
+                const float *e3 = g.e3;
                 float2 acc_r = make_float2(0.f, 0.f), acc_i = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int i = 0; i < kNuW; ++i) {
-                    float w = kEsTap[i][kEsDeg];
-#pragma unroll
-                    for (int q = kEsDeg - 1; q >= 0; --q) w = fmaf(w, sfr, kEsTap[i][q]);
-                    const float4 e = row[ix + i];
-                    acc_r = __ffma2_rn(make_float2(w, w), make_float2(e.x, e.y), acc_r);
-                    acc_i = __ffma2_rn(make_float2(w, w), make_float2(e.z, e.w), acc_i);
+                    const float4 e = row[g.ix + i];
+                    acc_r = __ffma2_rn(make_float2(g.w[i], g.w[i]), make_float2(e.x, e.y), acc_r);
+                    acc_i = __ffma2_rn(make_float2(g.w[i], g.w[i]), make_float2(e.z, e.w), acc_i);
                 }
                 // rotate by the anchor e^{-2pi i d (1/lambda + J0 slope/c)}: .x c', .y c
                 const float2 an = cis_fp64_phase(-d * k0c);
@@ -263,11 +313,12 @@ struct NuVariant {
      reinterpret_cast<const void *>(&bp_bwd_pos_nufft_kernel<T, NT, false>),               \
      "interp_t" #T "_n" #NT "_s" #CAP}
 
-// At 64^3 voxels, 4096 antennas, 128 samples (position pass alone, with vote term):
-// 11.2, 12.0, 13.6, 12.0 ms in this order; the first is the default.
+// At 64^3 voxels, 4096 antennas, 128 samples (position pass alone; with vote term / image
+// loss only): 9.00/8.43, 9.64/8.16, 11.1/11.8, 10.7/9.85 ms in this order; the first is the
+// default.
 const NuVariant kNuVariants[] = {
-    MMN_NU_VARIANT(2, 256, 24),
     MMN_NU_VARIANT(2, 128, 24),
+    MMN_NU_VARIANT(2, 256, 24),
     MMN_NU_VARIANT(1, 256, 48),
     MMN_NU_VARIANT(1, 128, 16),
 };

@@ -1,21 +1,23 @@
 // es_taps.cuh -- generated by gen_es_taps.py; do not edit.
-// Tap weights of the exponential-of-semicircle kernel (W = 8, beta = 2.3 W) as
-// degree-8 polynomials in the fractional grid offset s: weight_i(s) =
-// sum_n kEsTap[i][n] s^n, tap i at z = s + W/2 - 1 - i.  Fit error 1.9e-08.
+// Exponential-of-semicircle kernel (W = 8, beta = 2.3 W): with t = s - 1/2 for the
+// fractional grid offset s, tap i (0..3) weighs P_i(t) and tap 7-i weighs P_i(-t),
+// P_i(t) = sum_n kEsEven[i][n] t^(2n) + t sum_n kEsOdd[i][n] t^(2n).  Fit error 1.9e-08.
 #pragma once
 
 namespace mmn {
 
-constexpr int kEsDeg = 8;
-__constant__ float kEsTap[8][9] = {
-    {1.970351906e-03f, -1.027731411e-02f, 2.289049327e-02f, -2.788657881e-02f, 1.925509796e-02f, -6.266211625e-03f, -5.363195087e-04f, 1.121356268e-03f, -2.708597458e-04f},
-    {8.499756455e-02f, -2.257369757e-01f, 2.245005369e-01f, -7.796121389e-02f, -2.725812234e-02f, 3.085192293e-02f, -6.352500524e-03f, -1.797700999e-03f, 7.268397021e-04f},
-    {5.575090051e-01f, -6.621629000e-01f, 4.010197520e-02f, 2.399869114e-01f, -6.978011131e-02f, -4.198610783e-02f, 2.299735323e-02f, -6.749968743e-04f, -9.935779963e-04f},
-    {1.000000000e+00f, 1.684364747e-06f, -5.750369430e-01f, 3.423328453e-04f, 1.546784937e-01f, 4.527803510e-03f, -3.407115117e-02f, 6.575506181e-03f, 4.913107841e-04f},
-    {5.575090051e-01f, 6.621600389e-01f, 4.011413455e-02f, -2.405674309e-01f, -6.921529770e-02f, 3.430007771e-02f, 2.571409196e-02f, -1.050599199e-02f, 4.913107841e-04f},
-    {8.499755710e-02f, 2.257387042e-01f, 2.244861424e-01f, 7.831281424e-02f, -2.792570181e-02f, -2.618271112e-02f, -9.547807276e-03f, 8.623620495e-03f, -9.935779963e-04f},
-    {1.970356330e-03f, 1.027660631e-02f, 2.289967425e-02f, 2.774099819e-02f, 1.967322640e-02f, 4.311778117e-03f, 1.415104256e-03f, -4.017016850e-03f, 7.268397021e-04f},
-    {1.401200578e-08f, 2.036082606e-06f, 1.883858022e-05f, 1.753737743e-04f, 1.665327291e-04f, 1.103793387e-03f, -2.708986576e-04f, 1.045521698e-03f, -2.708597458e-04f},
+constexpr int kEsEvenTerms = 5, kEsOddTerms = 4;
+__constant__ float kEsEven[4][5] = {
+    {7.544255641e-05f, 2.225094941e-03f, 5.299292039e-03f, 1.492409152e-03f, -2.708597458e-04f},
+    {1.765909046e-02f, 9.841921926e-02f, 2.136478946e-02f, -7.556576282e-03f, 7.268397021e-04f},
+    {2.611282766e-01f, 2.636119127e-01f, -9.580532461e-02f, 1.367981825e-02f, -9.935779963e-04f},
+    {8.656142354e-01f, -3.642575145e-01f, 6.914851069e-02f, -7.617705502e-03f, 4.913107841e-04f},
+};
+__constant__ float kEsOdd[4][4] = {
+    {-6.272384780e-04f, -4.403749947e-03f, -3.884068225e-03f, 3.791726340e-05f},
+    {-6.503747404e-02f, -7.388940454e-02f, 7.444368675e-03f, 1.109657809e-03f},
+    {-4.859053791e-01f, 4.973948374e-02f, 1.650717109e-02f, -4.649308510e-03f},
+    {-5.016627312e-01f, 2.510846555e-01f, -5.972506851e-02f, 8.540749550e-03f},
 };
 
 }  // namespace mmn

@@ -1,11 +1,13 @@
-"""Writes es_taps.cuh: the eight tap weights of the exponential-of-semicircle interpolation
-kernel used by the position pass (bp_pos_nufft.cu) as degree-8 polynomials in the
-fractional grid offset s in [0, 1).
+"""Writes es_taps.cuh: the tap weights of the exponential-of-semicircle interpolation kernel
+used by the position pass (bp_pos_nufft.cu), as polynomials in the fractional grid offset.
 
 Kernel: phi(z) = exp(beta (sqrt(1 - (2z/W)^2) - 1)) for |z| < W/2, W = 8, beta = 2.3 W.
-Tap i sits at z = s + W/2 - 1 - i.  Each tap is a least-squares fit on 4001 points of
-[0, 1]; the fit error is below 2e-8 (phi(0) = 1), the FP32 Horner evaluation's rounding
-about 1e-7.  Run:  python mmnorm_b200/csrc/gen_es_taps.py
+Tap i (0..7) sits at z = s + W/2 - 1 - i for the fractional offset s in [0, 1).  With
+t = s - 1/2, tap i is P_i(t) = phi(t + W/2 - 1/2 - i) and, phi being even, tap W-1-i is
+P_i(-t).  So only P_0..P_3 are fitted (degree 8, least squares on 4001 points of
+[-1/2, 1/2]) and stored as even and odd parts:  P_i(t) = E_i(t^2) + t O_i(t^2), which gives
+both taps of a mirror pair from one E and one O.  Fit error below 2e-8 (phi(0) = 1); the
+FP32 evaluation's rounding is about 1e-7.  Run:  python mmnorm_b200/csrc/gen_es_taps.py
 """
 import os
 
@@ -23,33 +25,40 @@ def es(z):
 
 
 def fit():
-    s = np.linspace(0.0, 1.0, 4001)
-    coefs, worst = [], 0.0
-    for i in range(W):
-        y = es(s + W / 2 - 1 - i)
-        c = np.polynomial.Polynomial.fit(s, y, DEG, domain=[0, 1], window=[0, 1]).coef
-        worst = max(worst, float(np.abs(np.polynomial.polynomial.polyval(s, c) - y).max()))
-        coefs.append(c.astype(np.float32))
-    return coefs, worst
+    t = np.linspace(-0.5, 0.5, 4001)
+    even, odd, worst = [], [], 0.0
+    for i in range(W // 2):
+        c = np.polynomial.Polynomial.fit(t, es(t + W / 2 - 0.5 - i), DEG,
+                                         domain=[-0.5, 0.5], window=[-0.5, 0.5]).coef
+        c = np.concatenate([c, np.zeros(DEG + 1 - len(c))])
+        for sign, tap in ((1.0, i), (-1.0, W - 1 - i)):
+            y = es(sign * t + W / 2 - 0.5 - i) if sign > 0 else es(t + W / 2 - 0.5 - tap)
+            worst = max(worst, float(np.abs(np.polynomial.polynomial.polyval(sign * t, c)
+                                            - y).max()))
+        even.append(c[0::2].astype(np.float32))
+        odd.append(c[1::2].astype(np.float32))
+    return even, odd, worst
 
 
 def main():
-    coefs, worst = fit()
+    even, odd, worst = fit()
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "es_taps.cuh")
+    ne, no = len(even[0]), len(odd[0])
     lines = [
         "// es_taps.cuh -- generated by gen_es_taps.py; do not edit.",
-        "// Tap weights of the exponential-of-semicircle kernel (W = %d, beta = 2.3 W) as" % W,
-        "// degree-%d polynomials in the fractional grid offset s: weight_i(s) =" % DEG,
-        "// sum_n kEsTap[i][n] s^n, tap i at z = s + W/2 - 1 - i.  Fit error %.1e." % worst,
+        "// Exponential-of-semicircle kernel (W = %d, beta = 2.3 W): with t = s - 1/2 for the" % W,
+        "// fractional grid offset s, tap i (0..%d) weighs P_i(t) and tap %d-i weighs P_i(-t)," % (W // 2 - 1, W - 1),
+        "// P_i(t) = sum_n kEsEven[i][n] t^(2n) + t sum_n kEsOdd[i][n] t^(2n).  Fit error %.1e." % worst,
         "#pragma once",
         "",
         "namespace mmn {",
         "",
-        "constexpr int kEsDeg = %d;" % DEG,
-        "__constant__ float kEsTap[%d][%d] = {" % (W, DEG + 1),
+        "constexpr int kEsEvenTerms = %d, kEsOddTerms = %d;" % (ne, no),
+        "__constant__ float kEsEven[%d][%d] = {" % (W // 2, ne),
     ]
-    for c in coefs:
-        lines.append("    {" + ", ".join("%.9ef" % float(v) for v in c) + "},")
+    lines += ["    {" + ", ".join("%.9ef" % float(v) for v in c) + "}," for c in even]
+    lines += ["};", "__constant__ float kEsOdd[%d][%d] = {" % (W // 2, no)]
+    lines += ["    {" + ", ".join("%.9ef" % float(v) for v in c) + "}," for c in odd]
     lines += ["};", "", "}  // namespace mmn", ""]
     with open(out, "w") as f:
         f.write("\n".join(lines))
