@@ -574,25 +574,31 @@ def time_adjoint(dev):
                                                    pos_offsets=pos, want_pos=False))
     bwd_p = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
                                                    pos_offsets=pos, want_meas=False))
-    # a loss on the image only (no vote term): the position pass skips the vote terms
+    # a loss on the image only (no vote term): the passes skip the vote terms
     bwd_i = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, None,
                                                    pos_offsets=pos))
-    # the position pass's Horner form (two FP32 chains over all samples), for comparison
+    # both passes in their sum-over-samples / sum-over-voxels forms, for comparison
     ops.set_position_pass("horner")
+    ops.set_measurement_pass("horner")
     try:
         hor = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
                                                      pos_offsets=pos))
+        hor_m = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
+                                                       pos_offsets=pos, want_pos=False))
         hor_p = timed(lambda: ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, gW,
                                                        pos_offsets=pos, want_meas=False))
     finally:
         ops.set_position_pass("interp")
+        ops.set_measurement_pass("interp")
     return {"workload": sc.name + " (64^3 voxels @3 mm, 64x64 antennas @3 mm, 128 freqs)",
             "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
             "backward_meas_ms": bwd_m, "backward_pos_ms": bwd_p,
-            "position_pass": "interpolation (8-cell kernel, 2x oversampled per-antenna grid)",
+            "passes": "interpolation form (8-cell kernel, 2x oversampled per-antenna grids): "
+                      "type-2 gather for the position pass, type-1 spread for the "
+                      "measurement pass",
             "backward_image_loss_ms": bwd_i, "backward_image_loss_over_forward": bwd_i / fwd,
-            "horner_position_pass": {"backward_ms": hor, "backward_pos_ms": hor_p,
-                                     "backward_over_forward": hor / fwd}}
+            "horner_passes": {"backward_ms": hor, "backward_meas_ms": hor_m,
+                              "backward_pos_ms": hor_p, "backward_over_forward": hor / fwd}}
 
 
 def time_batched(dev, replays=3):

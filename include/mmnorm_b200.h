@@ -120,9 +120,19 @@ int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
  * used when F <= ~1500; MMN_POS_HORNER: two FP32 Horner chains over all F samples, as the
  * forward evaluates its sum.  Process-wide; the measurement gradient is the same in both.
  */
-#define MMN_POS_INTERP 0
-#define MMN_POS_HORNER 1
+#define MMN_PASS_INTERP 0
+#define MMN_PASS_HORNER 1
+#define MMN_POS_INTERP MMN_PASS_INTERP
+#define MMN_POS_HORNER MMN_PASS_HORNER
 int mmn_set_position_pass(int32_t form);
+/*
+ * The same choice for the measurement gradient dL/dm[a,j] = sum_v G conj(p) (no reference
+ * counterpart): MMN_PASS_INTERP (the default) spreads each voxel onto 8 cells of the
+ * antenna's oversampled grid and transforms each grid back to the F samples (type-1
+ * non-uniform FFT, deterministic warp reductions; F up to ~1500); MMN_PASS_HORNER sums
+ * over voxels for every sample.  Process-wide.
+ */
+int mmn_set_measurement_pass(int32_t form);
 /* Launch shapes of the interpolation form (voxels per thread, threads, stage size) for the
  * autotuner; process-wide, like mmn_set_variant. */
 int mmn_num_position_variants(void);

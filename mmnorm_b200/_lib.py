@@ -94,6 +94,7 @@ SIGNATURES = [
     ("mmn_backproject_noalloc", _I, [_PROB, _I32, _P, _P, _P]),
     ("mmn_backward_workspace_bytes", _SZ, [_PROB]),
     ("mmn_set_position_pass", _I, [_I32]),
+    ("mmn_set_measurement_pass", _I, [_I32]),
     ("mmn_num_position_variants", _I, []),
     ("mmn_position_variant_name", ctypes.c_char_p, [_I32]),
     ("mmn_set_position_variant", _I, [_I32]),

@@ -1,6 +1,6 @@
-// bp_pos_nufft.cu -- position pass of the adjoint in interpolation form.
+// bp_adjoint_nufft.cu -- the adjoint's two passes in interpolation form.
 //
-// The position gradient needs, per (voxel v, antenna a), the two sample sums
+// Position pass.  The position gradient needs, per (voxel v, antenna a), the two sums
 //   c_a(v)  = sum_j m[a,j] p_aj(v),   c'_a(v) = sum_j kappa_j m[a,j] p_aj(v),
 //   p_aj = exp(-i d kappa_j),  kappa_j = 2pi(1/lambda + j slope/c).
 // Both are one antenna's discrete-time Fourier sum evaluated at the point
@@ -15,11 +15,23 @@
 // (G'.re, G.re, G'.im, G.im) and two FFMA2 each -- in place of two F-step Horner chains.
 // Accuracy ~1e-7 relative (the FP32 Horner chains' level).
 //
+// Measurement pass.  dL/dm[a, J0+j'] = sum_v G_a(v) conj(p) = sum_v h_v e^{2pi i j' u_v} with
+// h_v = G_a(v) conj(anchor): the transposed (type-1) transform.  Each voxel spreads
+// h_v phi(N u_v - k) onto the same 8 cells it would read, the cells are summed over all
+// voxels into the antenna's grid S_k, and dL/dm[a, J0+j'] = sum_k S_k e^{2pi i j' k/N} /
+// phihat(j'/N) per antenna.  The spread is summed without atomics (deterministic): a warp
+// owns one antenna's grid row; each lane writes its 8 weighted cells into its own
+// 16-cell window in shared memory at its offset from the warp's lowest cell, and one
+// XOR-permuted transpose-reduce (31 shuffles) leaves cell j/2 of the window summed over
+// the warp in lane j.  Lanes whose cells fall outside a 16-cell window wait for the next
+// round, so any spread of distances is handled.
+//
 // Kernels: nufft_tables_kernel (1/phihat by midpoint quadrature in FP64, twiddles),
 // nufft_grid_kernel (per-antenna grids by a direct FP64 transform: F x (N + W - 1) per
 // antenna, small next to the voxel work), bp_bwd_pos_nufft_kernel (the forward's tiling and
 // double-buffered antenna staging, rows of N + W - 1 cells so no tap wraps; per-antenna
-// sums over a CTA's voxels go to the same per-tile partials as the Horner form).
+// sums over a CTA's voxels go to the same per-tile partials as the Horner form),
+// nufft_vox_kernel + bp_bwd_meas_nufft_kernel + nufft_meas_out_kernel (measurement pass).
 #include <algorithm>
 
 #include "bp_stage.cuh"
@@ -324,6 +336,188 @@ const NuVariant kNuVariants[] = {
 };
 #undef MMN_NU_VARIANT
 
+// ------------------------------------------------------------- measurement pass
+
+// Voxel records of the measurement pass, 5 x 16 bytes: (x, y) and (z, 0) in FP64, (x, y, z)
+// in FP32, (gI, gW_x), (gW_y, gW_z).
+__global__ void nufft_vox_kernel(const FwdParams p, const float2 *__restrict__ grad_image,
+                                 const float2 *__restrict__ grad_vote, float4 *__restrict__ rec) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= p.nvox) return;
+    const int64_t nyz = (int64_t)p.ny * p.nz;
+    const int ix = (int)(v / nyz);
+    const int64_t rem = v - (int64_t)ix * nyz;
+    const int iy = (int)(rem / p.nz);
+    const int iz = (int)(rem - (int64_t)iy * p.nz);
+    const float x = p.x_locs[ix], y = p.y_locs[iy], z = p.z_locs[iz];
+    const float2 gi = grad_image ? grad_image[v] : make_float2(0.f, 0.f);
+    float2 gw[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    if (grad_vote)
+        for (int k = 0; k < 3; ++k) gw[k] = grad_vote[k * p.nvox + v];
+    float4 *r = rec + 5 * v;
+    reinterpret_cast<double2 *>(r)[0] = make_double2(x, y);
+    reinterpret_cast<double2 *>(r)[1] = make_double2(z, 0.0);
+    r[2] = make_float4(x, y, z, 0.f);
+    r[3] = make_float4(gi.x, gi.y, gw[0].x, gw[0].y);
+    r[4] = make_float4(gw[1].x, gw[1].y, gw[2].x, gw[2].y);
+}
+
+constexpr int kNuMeasWarps = 4;
+constexpr int kNuScr = 17;  // float2 window slots per lane: 16 cells + 1 against bank conflicts
+
+// blockIdx.x = antenna group (one antenna per warp) + groups * voxel range.
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) bp_bwd_meas_nufft_kernel(const NuMeasParams q) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int groups = (q.num_ant + NW - 1) / NW;
+    const int g = blockIdx.x % groups;
+    const int range = blockIdx.x / groups;
+    const int a = g * NW + warp;
+    if (a >= q.num_ant) return;  // warps are independent: no block-wide barrier below
+    float2 *row = reinterpret_cast<float2 *>(smem) + (size_t)warp * (q.mrow + 32 * kNuScr);
+    float2 *scr = row + q.mrow + lane * kNuScr;
+    float *rowf = reinterpret_cast<float *>(row);
+    for (int c = lane; c < q.mrow; c += 32) row[c] = make_float2(0.f, 0.f);
+    __syncwarp();
+
+    const AntRec ar = q.ant[a];
+    const float txf[3] = {(float)ar.tx[0], (float)ar.tx[1], (float)ar.tx[2]};
+    const float rxf[3] = {(float)ar.rx[0], (float)ar.rx[1], (float)ar.rx[2]};
+    const bool mono = *q.mono_flag != 0;
+    const bool odd = lane & 1;
+    const int64_t v0 = (int64_t)range * q.vox_per_range;
+    const int64_t v1 = min(q.nvox, v0 + q.vox_per_range);
+
+    for (int64_t vb = v0; vb < v1; vb += 32) {
+        const int64_t v = vb + lane;
+        const bool ok = v < v1;
+        const float4 *r = q.vox + 5 * (ok ? v : v0);
+        const double2 xy = reinterpret_cast<const double2 *>(r)[0];
+        const double2 zz = reinterpret_cast<const double2 *>(r)[1];
+        const float4 fx = r[2], g0 = r[3], g1 = r[4];
+        NuPair pr;
+        nufft_pair(xy.x, xy.y, zz.x, fx.x, fx.y, fx.z, ar, txf, rxf, mono, q.ti, q.uq, q.n, pr);
+        const float2 an = cis_fp64_phase(-pr.d * q.k0c);
+        // G = gI + gW . (virt - v);  h = G conj(anchor), stored (re, im) on even lanes and
+        // (im, re) on odd lanes, the order the transpose-reduce reads them in
+        const float u0 = ar.virt[0] - fx.x, u1 = ar.virt[1] - fx.y, u2 = ar.virt[2] - fx.z;
+        float Gr = fmaf(g0.z, u0, g0.x), Gi = fmaf(g0.w, u0, g0.y);
+        Gr = fmaf(g1.x, u1, Gr);
+        Gi = fmaf(g1.y, u1, Gi);
+        Gr = fmaf(g1.z, u2, Gr);
+        Gi = fmaf(g1.w, u2, Gi);
+        const float hr = fmaf(Gr, an.x, Gi * an.y), hi = fmaf(Gi, an.x, -Gr * an.y);
+        const float h0 = odd ? hi : hr, h1 = odd ? hr : hi;
+        const int ix = pr.ix;
+
+        unsigned pending = __ballot_sync(0xffffffffu, ok);
+        while (pending) {
+            const bool mine_p = (pending >> lane) & 1u;
+            const int base = __reduce_min_sync(0xffffffffu, mine_p ? ix : 0x7fffffff);
+            const int off = ix - base;
+            const bool mine = mine_p && off <= 8;
+            if (mine) {
+#pragma unroll
+                for (int i = 0; i < kNuW; ++i)
+                    scr[off + i] = make_float2(h0 * pr.w[i], h1 * pr.w[i]);
+            }
+            __syncwarp();
+            // slot s holds window component s ^ lane: component c = cell c/2, re/im c&1
+            float vv[32];
+#pragma unroll
+            for (int s2 = 0; s2 < 16; ++s2) {
+                const int cell = s2 ^ (lane >> 1);
+                const int i = cell - off;
+                float2 t = make_float2(0.f, 0.f);
+                if (mine && i >= 0 && i < kNuW) t = scr[cell];
+                vv[2 * s2] = t.x;
+                vv[2 * s2 + 1] = t.y;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int h = 16; h >= 1; h >>= 1) {
+#pragma unroll
+                for (int i = 0; i < h; ++i) vv[i] += __shfl_xor_sync(0xffffffffu, vv[i + h], h);
+            }
+            rowf[2 * (base + (lane >> 1)) + (lane & 1)] += vv[0];
+            __syncwarp();
+            pending &= ~__ballot_sync(0xffffffffu, mine);
+        }
+    }
+    float2 *dst = q.part + ((size_t)range * q.num_ant + a) * q.mrow;
+    for (int c = lane; c < q.mrow; c += 32) dst[c] = row[c];
+}
+
+// Per antenna (one block): S_k = sum over voxel ranges and over the row cells that wrap
+// onto cell k, then dL/dm[a, j] = sc[j] sum_k S_k e^{2pi i (j - J0) k / N} in FP64.
+__global__ void nufft_meas_out_kernel(const NuMeasParams q) {
+    extern __shared__ __align__(16) unsigned char smem_out[];
+    double2 *S = reinterpret_cast<double2 *>(smem_out);
+    const int a = blockIdx.x;
+    const int n = q.n;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double sr = 0.0, si = 0.0;
+        for (int r = 0; r < q.ranges; ++r) {
+            const float2 *row = q.part + ((size_t)r * q.num_ant + a) * q.mrow;
+            for (int jj = (k + kNuW / 2 - 1) % n; jj < q.mrow; jj += n) {
+                sr += row[jj].x;
+                si += row[jj].y;
+            }
+        }
+        S[k] = make_double2(sr, si);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < q.F; j += blockDim.x) {
+        const int step = ((j - q.J0) % n + n) % n;
+        int idx = 0;
+        double er = 0.0, ei = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double2 t = q.tw[idx];  // e^{-2pi i idx/N}; the transform needs its conjugate
+            const double2 sk = S[k];
+            er = fma(sk.x, t.x, fma(sk.y, t.y, er));
+            ei = fma(sk.y, t.x, fma(-sk.x, t.y, ei));
+            idx += step;
+            if (idx >= n) idx -= n;
+        }
+        const double sc = q.sc[j];
+        q.grad_meas[(size_t)a * q.F + j] = make_float2((float)(er * sc), (float)(ei * sc));
+    }
+}
+
+size_t nufft_meas_smem(int mrow) {
+    return (size_t)kNuMeasWarps * (mrow + 32 * kNuScr) * sizeof(float2);
+}
+
+int nufft_meas_warps() { return kNuMeasWarps; }
+
+const void *nufft_meas_kernel_ptr() {
+    return reinterpret_cast<const void *>(&bp_bwd_meas_nufft_kernel<kNuMeasWarps>);
+}
+
+cudaError_t launch_nufft_meas(const NuMeasParams &q, const FwdParams &p,
+                              const float2 *grad_image, const float2 *grad_vote, float4 *rec,
+                              cudaStream_t stream) {
+    const int nt = 256;
+    nufft_vox_kernel<<<(unsigned)((p.nvox + nt - 1) / nt), nt, 0, stream>>>(p, grad_image,
+                                                                             grad_vote, rec);
+    const size_t smem = nufft_meas_smem(q.mrow);
+    const void *fn = nufft_meas_kernel_ptr();
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int groups = (q.num_ant + kNuMeasWarps - 1) / kNuMeasWarps;
+    void *args[] = {const_cast<NuMeasParams *>(&q)};
+    cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)((int64_t)groups * q.ranges)),
+                                     dim3(kNuMeasWarps * 32), args, smem, stream);
+    if (e != cudaSuccess) return e;
+    const size_t osmem = (size_t)q.n * sizeof(double2);
+    if (osmem > 48 * 1024)
+        cudaFuncSetAttribute(reinterpret_cast<const void *>(&nufft_meas_out_kernel),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)osmem);
+    nufft_meas_out_kernel<<<q.num_ant, 256, osmem, stream>>>(q);
+    return cudaGetLastError();
+}
+
 int bwd_pos_nufft_num_variants() { return (int)(sizeof(kNuVariants) / sizeof(kNuVariants[0])); }
 
 const char *bwd_pos_nufft_variant_name(int variant) {
@@ -341,13 +535,19 @@ const void *bwd_pos_nufft_kernel_ptr(int variant, bool vote, int *threads, int *
     return vote ? v.fn_vote : v.fn_img;
 }
 
-cudaError_t launch_nufft_grid(const float *meas, int A, int F, int N, int J0, double k0,
-                              double kd, double *sc, double2 *tw, float4 *rows,
-                              cudaStream_t stream) {
+cudaError_t launch_nufft_tables(int F, int N, int J0, double *sc, double2 *tw,
+                                cudaStream_t stream) {
     const int nt = 256;
     const int64_t tthreads = std::max<int64_t>((int64_t)F * 32, N);
     nufft_tables_kernel<<<(unsigned)((tthreads + nt - 1) / nt), nt, 0, stream>>>(F, N, J0, sc,
                                                                                  tw);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_nufft_grid(const float *meas, int A, int F, int N, int J0, double k0,
+                              double kd, const double *sc, const double2 *tw, float4 *rows,
+                              cudaStream_t stream) {
+    const int nt = 256;
     const int row = nufft_row(N);
     const int bpr = (row + nt - 1) / nt;
     nufft_grid_kernel<<<(unsigned)((int64_t)A * bpr), nt, 0, stream>>>(

@@ -85,7 +85,7 @@ struct BwdParams {
     double nu_k0c;             // 2pi (1/lambda + J0 slope/c), J0 = F/2: anchor phase per metre
 };
 
-// Interpolation-form position pass (bp_pos_nufft.cu): kernel width in grid cells, and the
+// Interpolation-form position pass (bp_adjoint_nufft.cu): kernel width in grid cells, and the
 // length of one antenna's staged grid row (N + W - 1 cells, so that no tap run wraps).
 constexpr int kNuW = 8;
 __host__ __device__ constexpr int nufft_row(int n) { return n + kNuW - 1; }
@@ -107,9 +107,30 @@ const void *bwd_pos_img_kernel_ptr(int *threads, int *voxels_per_thread);
 const void *bwd_pos_nufft_kernel_ptr(int variant, bool vote, int *threads, int *voxels_per_thread,
                                      int *stage_cap_bytes);
 int bwd_pos_nufft_num_variants();
+// Interpolation-form measurement pass.
+struct NuMeasParams {
+    const AntRec *ant;
+    const float4 *vox;        // [nvox][5] records (nufft_vox_kernel)
+    const int32_t *mono_flag;
+    float2 *part;             // [ranges][num_ant][mrow] per-range antenna grids
+    const double *sc;         // [F] 1/phihat((j - J0)/N)
+    const double2 *tw;        // [N] e^{-2pi i k/N}
+    float2 *grad_meas;        // [num_ant][F]
+    int64_t nvox, vox_per_range;
+    double ti, uq, k0c;       // 0.15 or 0; slope/c; 2pi(1/lambda + J0 slope/c)
+    int32_t num_ant, n, mrow, ranges, F, J0;  // mrow = N + 16 cells
+};
+size_t nufft_meas_smem(int mrow);
+int nufft_meas_warps();
+const void *nufft_meas_kernel_ptr();
+cudaError_t launch_nufft_meas(const NuMeasParams &q, const FwdParams &p,
+                              const float2 *grad_image, const float2 *grad_vote, float4 *rec,
+                              cudaStream_t stream);
 const char *bwd_pos_nufft_variant_name(int variant);  // null for a bad index
+cudaError_t launch_nufft_tables(int F, int N, int J0, double *sc, double2 *tw,
+                                cudaStream_t stream);
 cudaError_t launch_nufft_grid(const float *meas, int A, int F, int N, int J0, double k0,
-                              double kd, double *sc, double2 *tw, float4 *rows,
+                              double kd, const double *sc, const double2 *tw, float4 *rows,
                               cudaStream_t stream);
 
 // ---------------------------------------------------------- interpolated mode

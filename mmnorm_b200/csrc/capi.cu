@@ -584,32 +584,38 @@ int mmn_read_status(void *workspace, int32_t *status, cudaStream_t stream) {
 namespace {
 
 std::atomic<int> g_bwd_variant{0};
-std::atomic<int> g_pos_form{MMN_POS_INTERP};
+std::atomic<int> g_pos_form{MMN_PASS_INTERP};
 std::atomic<int> g_pos_variant{0};
+std::atomic<int> g_meas_form{MMN_PASS_INTERP};
 
 struct BwdPlan {
     int fp, ant_per_stage, tiles, splits, ant_per_split, threads, vpt;
     size_t smem;
-    size_t off_ant, off_meas, off_vox, off_pos, off_mpart, off_nutab, total;
+    size_t off_ant, off_meas, off_vox, off_pos, off_mpart, off_nutab, off_nvox, off_npart, total;
     int meas_splits;
     int64_t vox_per_split;
     const void *fn;
-    bool nufft;  // position pass in interpolation form
+    bool nufft;       // position pass in interpolation form
+    bool meas_nufft;  // measurement pass in interpolation form
     int nu_n, row;
+    int mrow, mranges;
+    int64_t mvox_per_range;
 };
 
 // image_only: the loss has no vote term (grad_vote NULL): the Horner form needs one chain
 // per voxel-antenna and runs the voxel-pair kernel; the interpolation form skips the vote
-// terms.  form: MMN_POS_INTERP (used when one staged grid row fits a shared-memory stage,
-// i.e. F up to about 1500) or MMN_POS_HORNER.
-int plan_backward(const mmn_problem *p, bool image_only, int form, BwdPlan *pl) {
+// terms.  form / meas_form: MMN_PASS_INTERP for the position / measurement pass (used when
+// one staged grid row fits a shared-memory stage, i.e. F up to about 1500) or MMN_PASS_HORNER.
+int plan_backward(const mmn_problem *p, bool image_only, int form, int meas_form,
+                  BwdPlan *pl) {
     const int A = p->num_antennas;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     pl->fp = (p->num_samples + kBlockF - 1) / kBlockF * kBlockF;
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
     pl->nu_n = 2 * p->num_samples;
-    pl->nufft = form == MMN_POS_INTERP &&
-                (int)sizeof(AntRec) + nufft_row(pl->nu_n) * 16 <= kMaxStageBytes;
+    const bool nu_fits = (int)sizeof(AntRec) + nufft_row(pl->nu_n) * 16 <= kMaxStageBytes;
+    pl->nufft = form == MMN_PASS_INTERP && nu_fits;
+    pl->meas_nufft = meas_form == MMN_PASS_INTERP && nu_fits;
     int cap = kMaxStageBytes;
     if (pl->nufft) {
         pl->fn = bwd_pos_nufft_kernel_ptr(g_pos_variant.load(), !image_only, &pl->threads,
@@ -661,9 +667,34 @@ int plan_backward(const mmn_problem *p, bool image_only, int form, BwdPlan *pl) 
     pl->off_meas = off;
     off = align_up(off + (size_t)A * pl->row * 16);
     pl->off_nutab = off;  // interpolation form: twiddles [N] double2, then 1/phihat [F] doubles
-    if (pl->nufft)
+    if (pl->nufft || pl->meas_nufft)
         off = align_up(off + (size_t)p->num_samples * sizeof(double) +
                        (size_t)pl->nu_n * sizeof(double2));
+    pl->off_nvox = pl->off_npart = off;
+    if (pl->meas_nufft) {
+        // voxel ranges: enough (antenna group, range) CTAs for two waves
+        pl->mrow = pl->nu_n + 16;
+        const size_t msmem = nufft_meas_smem(pl->mrow);
+        const void *mfn = nufft_meas_kernel_ptr();
+        if (msmem > 48 * 1024)
+            cudaFuncSetAttribute(mfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem);
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mfn, nufft_meas_warps() * 32,
+                                                          msmem) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        const int64_t groups = (A + nufft_meas_warps() - 1) / nufft_meas_warps();
+        const int64_t want = (2 * (int64_t)sms * per_sm + groups - 1) / std::max<int64_t>(groups, 1);
+        const int64_t chunks = std::max<int64_t>(1, (nvox + 31) / 32);
+        const int64_t ranges = std::max<int64_t>(1, std::min<int64_t>({want, 64, chunks}));
+        pl->mvox_per_range = (chunks + ranges - 1) / ranges * 32;
+        pl->mranges = (int)std::max<int64_t>(1, (nvox + pl->mvox_per_range - 1) / pl->mvox_per_range);
+        off = align_up(off + (size_t)nvox * 5 * sizeof(float4));
+        pl->off_npart = off;
+        off = align_up(off + (size_t)pl->mranges * A * pl->mrow * sizeof(float2));
+    }
     pl->off_vox = off;
     off = align_up(off + (size_t)nvox * 3 * sizeof(float4));
     pl->off_pos = off;
@@ -685,16 +716,24 @@ extern "C" size_t mmn_backward_workspace_bytes(const mmn_problem *p) {
     if (check_problem(p, MMN_MODE_MIXED) != MMN_OK) return 0;
     size_t total = 0;
     for (int form = 0; form < 2; ++form) {
-        BwdPlan pl, pl_img;
-        if (plan_backward(p, false, form, &pl) != MMN_OK) return 0;
-        if (plan_backward(p, true, form, &pl_img) != MMN_OK) return 0;
-        total = std::max(total, std::max(pl.total, pl_img.total));
+        for (int mform = 0; mform < 2; ++mform) {
+            BwdPlan pl, pl_img;
+            if (plan_backward(p, false, form, mform, &pl) != MMN_OK) return 0;
+            if (plan_backward(p, true, form, mform, &pl_img) != MMN_OK) return 0;
+            total = std::max(total, std::max(pl.total, pl_img.total));
+        }
     }
     return total;
 }
 
+extern "C" int mmn_set_measurement_pass(int32_t form) {
+    if (form != MMN_PASS_INTERP && form != MMN_PASS_HORNER) return MMN_ERR_INVALID_ARGUMENT;
+    g_meas_form.store(form);
+    return MMN_OK;
+}
+
 extern "C" int mmn_set_position_pass(int32_t form) {
-    if (form != MMN_POS_INTERP && form != MMN_POS_HORNER) return MMN_ERR_INVALID_ARGUMENT;
+    if (form != MMN_PASS_INTERP && form != MMN_PASS_HORNER) return MMN_ERR_INVALID_ARGUMENT;
     g_pos_form.store(form);
     return MMN_OK;
 }
@@ -726,7 +765,7 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     if (A == 0) return MMN_OK;
     const bool image_only = grad_vote == nullptr;
     BwdPlan pl;
-    rc = plan_backward(p, image_only, g_pos_form.load(), &pl);
+    rc = plan_backward(p, image_only, g_pos_form.load(), g_meas_form.load(), &pl);
     if (rc != MMN_OK) return rc;
     if (workspace_bytes < pl.total) return MMN_ERR_WORKSPACE;
     unsigned char *ws = static_cast<unsigned char *>(workspace);
@@ -775,10 +814,13 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     bp.meas_splits = pl.meas_splits;
     bp.meas_partial = reinterpret_cast<float2 *>(ws + pl.off_mpart);
     bp.vox_per_split = pl.vox_per_split;
+    const int J0 = F / 2;
+    double2 *tw = reinterpret_cast<double2 *>(ws + pl.off_nutab);  // 256-aligned
+    double *sc = reinterpret_cast<double *>(tw + pl.nu_n);
+    if (((grad_pos && pl.nufft) || (grad_meas && pl.meas_nufft)) &&
+        launch_nufft_tables(F, pl.nu_n, J0, sc, tw, stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
     if (grad_pos && pl.nufft) {
-        const int J0 = F / 2;
-        double2 *tw = reinterpret_cast<double2 *>(ws + pl.off_nutab);  // 256-aligned
-        double *sc = reinterpret_cast<double *>(tw + pl.nu_n);
         if (launch_nufft_grid(p->meas, A, F, pl.nu_n, J0, f.k0, f.kd, sc, tw,
                               reinterpret_cast<float4 *>(ws + pl.off_meas), stream) != cudaSuccess)
             return MMN_ERR_CUDA;
@@ -805,7 +847,32 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
             return MMN_ERR_CUDA;
         if (launch_bwd_pos_reduce(bp, stream) != cudaSuccess) return MMN_ERR_CUDA;
     }
-    if (grad_meas) {
+    if (grad_meas && pl.meas_nufft) {
+        NuMeasParams q;
+        std::memset(&q, 0, sizeof(q));
+        q.ant = ant;
+        q.vox = reinterpret_cast<const float4 *>(ws + pl.off_nvox);
+        q.mono_flag = hdr + 1;
+        q.part = reinterpret_cast<float2 *>(ws + pl.off_npart);
+        q.sc = sc;
+        q.tw = tw;
+        q.grad_meas = reinterpret_cast<float2 *>(grad_meas);
+        q.nvox = f.nvox;
+        q.vox_per_range = pl.mvox_per_range;
+        q.ti = f.ti;
+        q.uq = p->slope / kC;
+        q.k0c = 2.0 * kPi * (1.0 / p->wavelength + (double)J0 * p->slope / kC);
+        q.num_ant = A;
+        q.n = pl.nu_n;
+        q.mrow = pl.mrow;
+        q.ranges = pl.mranges;
+        q.F = F;
+        q.J0 = J0;
+        if (launch_nufft_meas(q, f, reinterpret_cast<const float2 *>(grad_image),
+                              reinterpret_cast<const float2 *>(grad_vote),
+                              reinterpret_cast<float4 *>(ws + pl.off_nvox), stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+    } else if (grad_meas) {
         if (launch_bwd_vox_rec(bp, reinterpret_cast<float4 *>(ws + pl.off_vox), stream) !=
             cudaSuccess)
             return MMN_ERR_CUDA;

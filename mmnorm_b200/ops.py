@@ -227,6 +227,14 @@ def set_position_pass(form):
     _lib.check(_lib.load().mmn_set_position_pass(POSITION_PASSES[form]), "mmn_set_position_pass")
 
 
+def set_measurement_pass(form):
+    """How the backward evaluates the measurement gradient: "interp" (default; spread onto
+    each antenna's 2x oversampled grid, then one transform per antenna; F <= ~1500) or
+    "horner" (a sum over voxels for every sample).  Process-wide."""
+    _lib.check(_lib.load().mmn_set_measurement_pass(POSITION_PASSES[form]),
+               "mmn_set_measurement_pass")
+
+
 def position_variants():
     """Launch shapes of the interpolation-form position pass, by index."""
     lib = _lib.load()

@@ -89,7 +89,15 @@ def pos_form(request):
     ops.set_position_pass("interp")
 
 
-def test_adjoint_matches_oracle(cuda_dev, oracle, pos_form):
+@pytest.fixture(params=["horner", "interp"])
+def meas_form(request):
+    from mmnorm_b200 import ops
+    ops.set_measurement_pass(request.param)
+    yield request.param
+    ops.set_measurement_pass("interp")
+
+
+def test_adjoint_matches_oracle(cuda_dev, oracle, pos_form, meas_form):
     import torch
     from mmnorm_b200 import ops
     sc = scenes.sphere_scene(seed=41, n_ap=6, nf=40, n_vox=5, n_pts=10)
@@ -110,7 +118,7 @@ def test_adjoint_matches_oracle(cuda_dev, oracle, pos_form):
     assert oracle.rel_l2(gp.cpu().numpy(), gp_o) < 2e-4
 
 
-def test_gradients_vs_dense_fp64_and_finite_differences(cuda_dev, pos_form):
+def test_gradients_vs_dense_fp64_and_finite_differences(cuda_dev, pos_form, meas_form):
     import torch
     from mmnorm_b200 import ops
     sc, t, rng, n_true = _problem(cuda_dev)
@@ -178,7 +186,7 @@ def test_gradients_vs_dense_fp64_and_finite_differences(cuda_dev, pos_form):
     assert np.linalg.norm(adm - fdm) / np.linalg.norm(fdm) < 2e-3
 
 
-def test_adjoint_dot_product_identity(cuda_dev):
+def test_adjoint_dot_product_identity(cuda_dev, meas_form):
     """I is linear in the measurements, so for any gI: Re<gI, I(m)> = Re<dL/dm, m>."""
     import torch
     from mmnorm_b200 import ops
@@ -196,7 +204,7 @@ def test_adjoint_dot_product_identity(cuda_dev):
     assert abs(float(lhs - rhs)) <= 2e-5 * abs(float(lhs))
 
 
-def test_image_only_position_gradient(cuda_dev, oracle, pos_form):
+def test_image_only_position_gradient(cuda_dev, oracle, pos_form, meas_form):
     """Without a vote term the position pass skips the vote terms (Horner form: one chain
     per voxel-antenna, voxel pairs in the FFMA2 halves); it must agree with the oracle's
     adjoint and with the full kernel given an all-zero vote gradient."""
@@ -300,3 +308,46 @@ def test_position_variants_agree(cuda_dev, oracle):
         assert oracle.rel_l2(gp, gp_img if img else gp_o) < 2e-4, (names[i], img)
     with pytest.raises(Exception):
         ops.set_position_variant(len(names))
+
+
+@pytest.mark.parametrize("nf", [1, 3, 40, 129])
+@pytest.mark.parametrize("spacing", [None, 0.04])
+def test_interpolation_measurement_pass(cuda_dev, oracle, nf, spacing):
+    """The measurement gradient's interpolation form against the voxel-sum form and the
+    oracle, over sample counts down to one and on a sparse grid (4 cm voxel pitch: a warp's
+    32 voxels spread over ~80 grid cells, so its window reduction takes many rounds)."""
+    import torch
+    from mmnorm_b200 import ops
+    sc = scenes.sphere_scene(seed=60 + nf, n_ap=7, nf=max(nf, 2), n_vox=7, n_pts=12)
+    meas = np.ascontiguousarray(sc.meas[:, :nf])
+    x, y, z = sc.x_locs, sc.y_locs, sc.z_locs
+    if spacing is not None:
+        x = (x.mean() + spacing * (np.arange(5) - 2)).astype(np.float32)
+        y = (y.mean() + spacing * (np.arange(4) - 1.5)).astype(np.float32)
+        z = (z.mean() + spacing * (np.arange(40) - 19.5)).astype(np.float32)
+    rng = np.random.default_rng(60)
+    rxo = np.array([[0.0, -0.004, 0.001]], np.float32)
+    V = len(x) * len(y) * len(z)
+    gI = (rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64)
+    gW = (rng.standard_normal((3, V)) + 1j * rng.standard_normal((3, V))).astype(np.complex64)
+    args = [_t(a, cuda_dev) for a in (x, y, z, sc.antenna_locs, rxo, meas)]
+    out = {}
+    try:
+        for form in ("interp", "horner"):
+            ops.set_measurement_pass(form)
+            out[form] = ops.backproject_backward(*args, sc.wavelength, sc.slope,
+                                                 _t(gI, cuda_dev), _t(gW, cuda_dev),
+                                                 want_pos=False)[0]
+        ops.set_measurement_pass("interp")
+        again = ops.backproject_backward(*args, sc.wavelength, sc.slope, _t(gI, cuda_dev),
+                                         _t(gW, cuda_dev), want_pos=False)[0]
+    finally:
+        ops.set_measurement_pass("interp")
+    torch.cuda.synchronize()
+    assert torch.equal(out["interp"], again)  # no atomics: bitwise repeatable
+    vox = np.stack(np.meshgrid(x, y, z, indexing="ij"), -1).reshape(-1, 3)
+    gm_o, _ = oracle.full_backward(vox, sc.antenna_locs, rxo, meas, sc.wavelength, sc.slope,
+                                   gI.astype(np.complex128), gW.T.astype(np.complex128))
+    a, b = (out[f].cpu().numpy().astype(np.complex128) for f in ("interp", "horner"))
+    assert oracle.rel_l2(b, gm_o) < 2e-5
+    assert oracle.rel_l2(a, gm_o) < 2e-5
