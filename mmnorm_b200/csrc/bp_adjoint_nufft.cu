@@ -21,7 +21,8 @@
 // voxels into the antenna's grid S_k, and dL/dm[a, J0+j'] = sum_k S_k e^{2pi i j' k/N} /
 // phihat(j'/N) per antenna.  The spread is summed without atomics (deterministic): a warp
 // owns one antenna's grid row; each lane writes its 8 weighted cells into its own
-// 16-cell window in shared memory at its offset from the warp's lowest cell, and one
+// 16-cell window in shared memory (cell-major across the lanes: conflict-free) at its
+// offset from the warp's lowest cell, and one
 // XOR-permuted transpose-reduce (31 shuffles) leaves cell j/2 of the window summed over
 // the warp in lane j.  Lanes whose cells fall outside a 16-cell window wait for the next
 // round, so any spread of distances is handled.
@@ -363,7 +364,7 @@ __global__ void nufft_vox_kernel(const FwdParams p, const float2 *__restrict__ g
 }
 
 constexpr int kNuMeasWarps = 4;
-constexpr int kNuScr = 17;  // float2 window slots per lane: 16 cells + 1 against bank conflicts
+constexpr int kNuWin = 16;  // window cells per round
 
 // blockIdx.x = antenna group (one antenna per warp) + groups * voxel range.
 template <int NW>
@@ -375,8 +376,10 @@ __global__ void __launch_bounds__(NW * 32) bp_bwd_meas_nufft_kernel(const NuMeas
     const int range = blockIdx.x / groups;
     const int a = g * NW + warp;
     if (a >= q.num_ant) return;  // warps are independent: no block-wide barrier below
-    float2 *row = reinterpret_cast<float2 *>(smem) + (size_t)warp * (q.mrow + 32 * kNuScr);
-    float2 *scr = row + q.mrow + lane * kNuScr;
+    // per warp: its antenna's grid row, then the lanes' windows cell-major (cell * 32 + lane:
+    // every access of a half-warp falls in 16 different banks, whatever the cells)
+    float2 *row = reinterpret_cast<float2 *>(smem) + (size_t)warp * (q.mrow + 32 * kNuWin);
+    float2 *win = row + q.mrow + lane;
     float *rowf = reinterpret_cast<float *>(row);
     for (int c = lane; c < q.mrow; c += 32) row[c] = make_float2(0.f, 0.f);
     __syncwarp();
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(NW * 32) bp_bwd_meas_nufft_kernel(const NuMeas
             if (mine) {
 #pragma unroll
                 for (int i = 0; i < kNuW; ++i)
-                    scr[off + i] = make_float2(h0 * pr.w[i], h1 * pr.w[i]);
+                    win[(off + i) * 32] = make_float2(h0 * pr.w[i], h1 * pr.w[i]);
             }
             __syncwarp();
             // slot s holds window component s ^ lane: component c = cell c/2, re/im c&1
@@ -430,7 +433,7 @@ __global__ void __launch_bounds__(NW * 32) bp_bwd_meas_nufft_kernel(const NuMeas
                 const int cell = s2 ^ (lane >> 1);
                 const int i = cell - off;
                 float2 t = make_float2(0.f, 0.f);
-                if (mine && i >= 0 && i < kNuW) t = scr[cell];
+                if (mine && i >= 0 && i < kNuW) t = win[cell * 32];
                 vv[2 * s2] = t.x;
                 vv[2 * s2 + 1] = t.y;
             }
@@ -486,7 +489,7 @@ __global__ void nufft_meas_out_kernel(const NuMeasParams q) {
 }
 
 size_t nufft_meas_smem(int mrow) {
-    return (size_t)kNuMeasWarps * (mrow + 32 * kNuScr) * sizeof(float2);
+    return (size_t)kNuMeasWarps * (mrow + 32 * kNuWin) * sizeof(float2);
 }
 
 int nufft_meas_warps() { return kNuMeasWarps; }
