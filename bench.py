@@ -17,6 +17,7 @@ host cores on a bounded voxel sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -42,6 +43,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--nufft-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU seconds of the bounded reference/CPU sample")
@@ -269,12 +271,12 @@ def ours_arm(args):
 
     max_abs = torch.empty(1, dtype=torch.float32, device=dev)
 
-    def step(mode="mixed", ev=None):
+    def step(mode="mixed", ev=None, workspace=None):
         flush.fill_(1)
         if ev is not None:
             ev[0].record(stream)
         img, vote = ops.backproject(xs, ys, zs, ant, rxo, meas, sc.wavelength, sc.slope,
-                                    mode=mode, workspace=ws)
+                                    mode=mode, workspace=ws if workspace is None else workspace)
         if ev is not None:
             ev[1].record(stream)
         # mask threshold: 5 % of max|I| over the whole grid (one float all-reduced)
@@ -353,6 +355,36 @@ def ours_arm(args):
                         "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in pe),
                         "mixed_over_plain": value / pval,
                         "variant": ops.variants("plain")[ptuned["best"]]["name"]}
+
+    if rank == 0 and world == 1 and args.nufft_steps > 0:
+        # the same sums by 8-tap interpolation from per-antenna oversampled grids (a type-2
+        # non-uniform FFT): not the mixed recurrence, so reported beside it, with its
+        # distance from the mixed form's outputs on this workload
+        img_m, vote_m, _, _ = step()
+        img_m, vote_m = img_m.clone(), vote_m.clone()
+        ws_nu = torch.empty(lib.mmn_backproject_nufft_workspace_bytes(ctypes.byref(prob)),
+                            dtype=torch.uint8, device=dev)
+        img_n, vote_n, _, _ = step("nufft", workspace=ws_nu)
+        rel = lambda a, b: float((a.to(torch.complex128) - b.to(torch.complex128)).norm() /
+                                 b.to(torch.complex128).norm())
+        rel_img, rel_vote = rel(img_n, img_m), rel(vote_n, vote_m)
+        del img_m, vote_m, img_n, vote_n
+        ne = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.nufft_steps)]
+        torch.cuda.synchronize()
+        n0, n1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0.record(stream)
+        for k in range(args.nufft_steps):
+            step("nufft", ev=ne[k], workspace=ws_nu)
+        n1.record(stream)
+        torch.cuda.synchronize()
+        nms = n0.elapsed_time(n1) / args.nufft_steps
+        nval = updates / (nms * 1e-3) / 1e9
+        out["nufft"] = {"value": nval, "unit": UNIT + " equivalent (interpolated sums)",
+                        "ms_per_step": nms,
+                        "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in ne),
+                        "over_mixed": nval / value,
+                        "rel_l2_vs_mixed": {"image": rel_img, "vote": rel_vote}}
 
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:

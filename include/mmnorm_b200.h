@@ -140,6 +140,19 @@ const char *mmn_position_variant_name(int32_t idx); /* NULL for a bad index */
 int mmn_set_position_variant(int32_t idx);
 
 /*
+ * Fused backprojection + vote with the per-(voxel, antenna) sample sum evaluated by
+ * interpolation (no counterpart in the reference; not its "interpolated mode", which reads
+ * one range bin): each antenna's samples go once onto a 2x oversampled grid, and each
+ * (voxel, antenna) gathers 8 cells with exponential-of-semicircle weights -- a type-2
+ * non-uniform FFT, O(8) per pair instead of O(F).  Same outputs and problem fields as
+ * mmn_backproject in MMN_MODE_MIXED, ~1e-7 relative from it; F up to ~1500
+ * (MMN_ERR_TOO_LARGE above).  Needs mmn_backproject_nufft_workspace_bytes() of workspace.
+ */
+size_t mmn_backproject_nufft_workspace_bytes(const mmn_problem *p);
+int mmn_backproject_nufft(const mmn_problem *p, float *image, float *vote, void *workspace,
+                          size_t workspace_bytes, cudaStream_t stream);
+
+/*
  * Batched persistent launch (no counterpart in the reference, which images one object per
  * call; mmwave_reconstruction.sh:61-69 loops over objects in the shell).  Many objects --
  * each its own voxel grid, aperture, sample count and radar constants -- run in ONE

@@ -93,6 +93,8 @@ SIGNATURES = [
     ("mmn_backproject", _I, [_PROB, _I32, _P, _P, _P, _SZ, _P]),
     ("mmn_backproject_noalloc", _I, [_PROB, _I32, _P, _P, _P]),
     ("mmn_backward_workspace_bytes", _SZ, [_PROB]),
+    ("mmn_backproject_nufft_workspace_bytes", _SZ, [_PROB]),
+    ("mmn_backproject_nufft", _I, [_PROB, _P, _P, _P, _SZ, _P]),
     ("mmn_set_position_pass", _I, [_I32]),
     ("mmn_set_measurement_pass", _I, [_I32]),
     ("mmn_num_position_variants", _I, []),

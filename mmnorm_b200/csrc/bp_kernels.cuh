@@ -85,7 +85,7 @@ struct BwdParams {
     double nu_k0c;             // 2pi (1/lambda + J0 slope/c), J0 = F/2: anchor phase per metre
 };
 
-// Interpolation-form position pass (bp_adjoint_nufft.cu): kernel width in grid cells, and the
+// Interpolation-form position pass (bp_nufft.cu): kernel width in grid cells, and the
 // length of one antenna's staged grid row (N + W - 1 cells, so that no tap run wraps).
 constexpr int kNuW = 8;
 __host__ __device__ constexpr int nufft_row(int n) { return n + kNuW - 1; }
@@ -120,6 +120,8 @@ struct NuMeasParams {
     double ti, uq, k0c;       // 0.15 or 0; slope/c; 2pi(1/lambda + J0 slope/c)
     int32_t num_ant, n, mrow, ranges, F, J0;  // mrow = N + 16 cells
 };
+// forward in interpolation form (bp_fwd_nufft_kernel; BwdParams carries the nu fields)
+const void *fwd_nufft_kernel_ptr(int *threads, int *voxels_per_thread);
 size_t nufft_meas_smem(int mrow);
 int nufft_meas_warps();
 const void *nufft_meas_kernel_ptr();

@@ -1,4 +1,4 @@
-// bp_adjoint_nufft.cu -- the adjoint's two passes in interpolation form.
+// bp_nufft.cu -- the adjoint's two passes in interpolation form.
 //
 // Position pass.  The position gradient needs, per (voxel v, antenna a), the two sums
 //   c_a(v)  = sum_j m[a,j] p_aj(v),   c'_a(v) = sum_j kappa_j m[a,j] p_aj(v),
@@ -336,6 +336,109 @@ const NuVariant kNuVariants[] = {
     MMN_NU_VARIANT(1, 128, 16),
 };
 #undef MMN_NU_VARIANT
+
+// ---------------------------------------------------------------- forward pass
+// The forward's per-(voxel, antenna) sum c = sum_j m_j p_j by the same 8-tap gather as the
+// position pass (the rows' G cells), accumulated as I += c, W += c (virt - v) per voxel
+// over the CTA's antennas; results go through store_voxel (direct or per-split partials).
+template <int T, int NT>
+__global__ void __launch_bounds__(NT) bp_fwd_nufft_kernel(const BwdParams bp) {
+    const FwdParams &p = bp.f;
+    extern __shared__ __align__(128) unsigned char smem[];
+    Stage st;
+    st.bars = reinterpret_cast<uint64_t *>(smem);
+    st.base = smem + 128;
+    st.nas = p.ant_per_stage;
+    st.esz = 16;
+    st.fp = p.fp;  // grid row length N + W - 1
+    st.stage_bytes = (size_t)st.nas * sizeof(AntRec) + (size_t)st.nas * st.fp * st.esz;
+    const int row_len = p.fp;
+    const int n = bp.nu_n;
+    const double uq = bp.nu_u, k0c = bp.nu_k0c;
+    const int tile = blockIdx.x % p.num_tiles;
+    const int split = blockIdx.x / p.num_tiles;
+    const int a_begin = split * p.ant_per_split;
+    const int a_end = min(p.num_ant, a_begin + p.ant_per_split);
+    const int n_chunks = a_end > a_begin ? (a_end - a_begin + st.nas - 1) / st.nas : 0;
+
+    if (threadIdx.x == 0) {
+        mbar_init(&st.bars[0], 1);
+        mbar_init(&st.bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (n_chunks > 0) st.issue(p, 0, a_begin, a_end);
+        if (n_chunks > 1) st.issue(p, 1, a_begin, a_end);
+    }
+
+    const int64_t rbase = (int64_t)tile * (NT * T) + threadIdx.x;
+    float vx[T], vy[T], vz[T];
+    double vxd[T], vyd[T], vzd[T];
+    float acc[T][8];
+#pragma unroll
+    for (int k = 0; k < T; ++k) {
+        decode_voxel(p, rbase + (int64_t)k * NT, vx[k], vy[k], vz[k]);
+        vxd[k] = vx[k];
+        vyd[k] = vy[k];
+        vzd[k] = vz[k];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[k][q] = 0.f;
+    }
+    const bool mono = *p.mono_flag != 0;
+
+    for (int c = 0; c < n_chunks; ++c) {
+        const int s = c & 1;
+        bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
+        if (!__syncthreads_and(ok)) return;
+        const AntRec *ants = st.ants(s);
+        const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
+        const int a0 = a_begin + c * st.nas;
+        const int na = min(st.nas, a_end - a0);
+        for (int a = 0; a < na; ++a) {
+            const AntRec &ar = ants[a];
+            const float4 *row = mstage + (size_t)a * row_len;
+            const float txf[3] = {(float)ar.tx[0], (float)ar.tx[1], (float)ar.tx[2]};
+            const float rxf[3] = {(float)ar.rx[0], (float)ar.rx[1], (float)ar.rx[2]};
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                NuPair g;
+                nufft_pair(vxd[k], vyd[k], vzd[k], vx[k], vy[k], vz[k], ar, txf, rxf, mono, p.ti,
+                           uq, n, g);
+                float2 h = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int i = 0; i < kNuW; ++i) {
+                    const float4 e = row[g.ix + i];
+                    h = __ffma2_rn(make_float2(g.w[i], g.w[i]), make_float2(e.y, e.w), h);
+                }
+                const float2 an = cis_fp64_phase(-g.d * k0c);
+                const float cr = fmaf(an.x, h.x, -an.y * h.y), ci = fmaf(an.x, h.y, an.y * h.x);
+                const float u0 = ar.virt[0] - vx[k], u1 = ar.virt[1] - vy[k],
+                            u2 = ar.virt[2] - vz[k];
+                acc[k][0] += cr;
+                acc[k][1] += ci;
+                acc[k][2] = fmaf(cr, u0, acc[k][2]);
+                acc[k][3] = fmaf(ci, u0, acc[k][3]);
+                acc[k][4] = fmaf(cr, u1, acc[k][4]);
+                acc[k][5] = fmaf(ci, u1, acc[k][5]);
+                acc[k][6] = fmaf(cr, u2, acc[k][6]);
+                acc[k][7] = fmaf(ci, u2, acc[k][7]);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
+    }
+#pragma unroll
+    for (int k = 0; k < T; ++k) store_voxel(p, split, rbase + (int64_t)k * NT, acc[k]);
+}
+
+constexpr int kNuFwdT = 2, kNuFwdNT = 128;
+
+const void *fwd_nufft_kernel_ptr(int *threads, int *voxels_per_thread) {
+    *threads = kNuFwdNT;
+    *voxels_per_thread = kNuFwdT;
+    return reinterpret_cast<const void *>(&bp_fwd_nufft_kernel<kNuFwdT, kNuFwdNT>);
+}
 
 // ------------------------------------------------------------- measurement pass
 

@@ -726,6 +726,155 @@ extern "C" size_t mmn_backward_workspace_bytes(const mmn_problem *p) {
     return total;
 }
 
+// ---------------------------------------------------------------------------------
+// Forward in interpolation form: the per-(voxel, antenna) sample sum by an 8-tap gather
+// from each antenna's 2x oversampled grid (the position pass's machinery).
+// ---------------------------------------------------------------------------------
+namespace {
+
+struct NuFwdPlan {
+    int n, row, threads, vpt, ant_per_stage, tiles, splits, ant_per_split;
+    size_t smem, off_ant, off_rows, off_tab, off_part, total;
+    const void *fn;
+};
+
+int plan_nufft_forward(const mmn_problem *p, NuFwdPlan *pl) {
+    const int A = p->num_antennas, F = p->num_samples;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    pl->n = 2 * F;
+    pl->row = nufft_row(pl->n);
+    const int rec = (int)sizeof(AntRec) + pl->row * 16;
+    if (rec > kMaxStageBytes) return MMN_ERR_TOO_LARGE;
+    pl->fn = fwd_nufft_kernel_ptr(&pl->threads, &pl->vpt);
+    pl->ant_per_stage = std::max(1, std::min(16, 24 * 1024 / rec));
+    pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec;
+    const int64_t per_tile = (int64_t)pl->threads * pl->vpt;
+    const int64_t tiles = (nvox + per_tile - 1) / per_tile;
+    if (tiles > (int64_t)1 << 30) return MMN_ERR_TOO_LARGE;
+    pl->tiles = (int)std::max<int64_t>(1, tiles);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (pl->smem > 48 * 1024)
+        cudaFuncSetAttribute(pl->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl->smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pl->fn, pl->threads, pl->smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    const int64_t slots = (int64_t)sms * per_sm;
+    int best_s = 1;
+    double best_cost = 1e300;
+    const int max_s = std::max(1, std::min(64, (A + pl->ant_per_stage - 1) / pl->ant_per_stage));
+    for (int s = 1; s <= max_s; ++s) {
+        const int64_t ctas = (int64_t)pl->tiles * s;
+        const double waves = (double)((ctas + slots - 1) / slots);
+        const double cost = waves * std::ceil((double)A / s) * (1.0 + 0.02 * (s - 1));
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best_s = s;
+        }
+        if (ctas >= 8 * slots) break;
+    }
+    int aps = (A + best_s - 1) / best_s;
+    aps = (aps + pl->ant_per_stage - 1) / pl->ant_per_stage * pl->ant_per_stage;
+    pl->ant_per_split = std::max(aps, 1);
+    pl->splits = std::max(1, (A + pl->ant_per_split - 1) / pl->ant_per_split);
+    size_t off = kStatusBytes;
+    pl->off_ant = off;
+    off = align_up(off + (size_t)A * sizeof(AntRec));
+    pl->off_rows = off;
+    off = align_up(off + (size_t)A * pl->row * 16);
+    pl->off_tab = off;
+    off = align_up(off + (size_t)pl->n * sizeof(double2) + (size_t)F * sizeof(double));
+    pl->off_part = off;
+    if (pl->splits > 1) off = align_up(off + (size_t)pl->splits * nvox * 2 * sizeof(float4));
+    pl->total = off;
+    return MMN_OK;
+}
+
+}  // namespace
+
+extern "C" size_t mmn_backproject_nufft_workspace_bytes(const mmn_problem *p) {
+    if (check_problem(p, MMN_MODE_MIXED) != MMN_OK) return 0;
+    NuFwdPlan pl;
+    return plan_nufft_forward(p, &pl) == MMN_OK ? pl.total : 0;
+}
+
+extern "C" int mmn_backproject_nufft(const mmn_problem *p, float *image, float *vote,
+                                     void *workspace, size_t workspace_bytes,
+                                     cudaStream_t stream) {
+    int rc = check_problem(p, MMN_MODE_MIXED);
+    if (rc != MMN_OK) return rc;
+    if (!image) return MMN_ERR_NULL_POINTER;
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
+        return MMN_ERR_WORKSPACE;
+    if (reinterpret_cast<uintptr_t>(p->meas) & 7u) return MMN_ERR_INVALID_ARGUMENT;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    const int A = p->num_antennas, F = p->num_samples;
+    if (A == 0) {
+        if (cudaMemsetAsync(image, 0, nvox * 8, stream) != cudaSuccess) return MMN_ERR_CUDA;
+        if (vote && cudaMemsetAsync(vote, 0, 3 * nvox * 8, stream) != cudaSuccess)
+            return MMN_ERR_CUDA;
+        return MMN_OK;
+    }
+    NuFwdPlan pl;
+    rc = plan_nufft_forward(p, &pl);
+    if (rc != MMN_OK) return rc;
+    if (workspace_bytes < pl.total) return MMN_ERR_WORKSPACE;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    if (cudaMemsetAsync(ws, 0, 16, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    int32_t *hdr = reinterpret_cast<int32_t *>(ws);
+    AntRec *ant = reinterpret_cast<AntRec *>(ws + pl.off_ant);
+    if (launch_prep_antennas(p->antenna_locs, p->rx_offsets, p->num_rx, p->pos_offsets, A, A, ant,
+                             hdr + 1, stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    const int J0 = F / 2;
+    double2 *tw = reinterpret_cast<double2 *>(ws + pl.off_tab);
+    double *sc = reinterpret_cast<double *>(tw + pl.n);
+    const double k0 = 2.0 * kPi / p->wavelength, kd = 2.0 * kPi * p->slope / kC;
+    if (launch_nufft_tables(F, pl.n, J0, sc, tw, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    if (launch_nufft_grid(p->meas, A, F, pl.n, J0, k0, kd, sc, tw,
+                          reinterpret_cast<float4 *>(ws + pl.off_rows), stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    BwdParams bq;
+    std::memset(&bq, 0, sizeof(bq));
+    FwdParams &f = bq.f;
+    f.x_locs = p->x_locs;
+    f.y_locs = p->y_locs;
+    f.z_locs = p->z_locs;
+    f.nx = p->num_x;
+    f.ny = p->num_y;
+    f.nz = p->num_z;
+    f.nvox = nvox;
+    f.vox_start = 0;
+    f.vox_count = nvox;
+    f.ant = ant;
+    f.meas = ws + pl.off_rows;
+    f.num_ant = A;
+    f.fp = pl.row;
+    f.ant_per_stage = pl.ant_per_stage;
+    f.mono_flag = hdr + 1;
+    f.ti = p->is_ti_radar ? 0.15 : 0.0;
+    f.num_tiles = pl.tiles;
+    f.num_splits = pl.splits;
+    f.ant_per_split = pl.ant_per_split;
+    f.image = reinterpret_cast<float2 *>(image);
+    f.vote = reinterpret_cast<float2 *>(vote);
+    f.partial = reinterpret_cast<float4 *>(ws + pl.off_part);
+    f.status = hdr;
+    bq.nu_n = pl.n;
+    bq.nu_u = p->slope / kC;
+    bq.nu_k0c = 2.0 * kPi * (1.0 / p->wavelength + (double)J0 * p->slope / kC);
+    if (pl.smem > 48 * 1024)
+        cudaFuncSetAttribute(pl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem);
+    void *args[] = {&bq};
+    if (cudaLaunchKernel(pl.fn, dim3(pl.tiles * pl.splits), dim3(pl.threads), args, pl.smem,
+                         stream) != cudaSuccess)
+        return MMN_ERR_CUDA;
+    if (pl.splits > 1 && launch_reduce(f, stream) != cudaSuccess) return MMN_ERR_CUDA;
+    return MMN_OK;
+}
+
 extern "C" int mmn_set_measurement_pass(int32_t form) {
     if (form != MMN_PASS_INTERP && form != MMN_PASS_HORNER) return MMN_ERR_INVALID_ARGUMENT;
     g_meas_form.store(form);

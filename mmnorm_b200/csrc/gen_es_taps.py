@@ -1,5 +1,5 @@
 """Writes es_taps.cuh: the tap weights of the exponential-of-semicircle interpolation kernel
-used by the position pass (bp_adjoint_nufft.cu), as polynomials in the fractional grid offset.
+used by the position pass (bp_nufft.cu), as polynomials in the fractional grid offset.
 
 Kernel: phi(z) = exp(beta (sqrt(1 - (2z/W)^2) - 1)) for |z| < W/2, W = 8, beta = 2.3 W.
 Tap i (0..7) sits at z = s + W/2 - 1 - i for the fractional offset s in [0, 1).  With

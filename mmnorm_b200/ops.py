@@ -109,7 +109,9 @@ def backproject(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, waveleng
     Returns ``image`` complex64 [NX, NY, NZ] (raw sum over virtual antennas and samples,
     not normalised) and ``vote`` complex64 [3, NX, NY, NZ] (or None).
     ``mode``: 'mixed' (FP64 range/wrap + FP32 recurrence), 'plain' (FP32 sincos per
-    sample) or 'interp' (reference interpolated mode; ``meas`` holds range-FFT bins).
+    sample), 'interp' (reference interpolated mode; ``meas`` holds range-FFT bins) or
+    'nufft' (the mixed form's sum by an 8-tap gather from each antenna's 2x oversampled
+    grid, ~1e-7 from 'mixed', O(8) instead of O(F) per voxel and antenna; F <= ~1500).
     """
     meas = _plain(meas)
     p = make_problem(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength,
@@ -120,6 +122,16 @@ def backproject(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, waveleng
     image = torch.empty(V, dtype=torch.complex64, device=dev)
     vote = torch.empty((3, V), dtype=torch.complex64, device=dev) if want_vote else None
     lib = _lib.load()
+    if mode == "nufft":
+        nbytes = lib.mmn_backproject_nufft_workspace_bytes(ctypes.byref(p))
+        if nbytes == 0:
+            raise _lib.MmnError(_lib.MMN_ERR_TOO_LARGE, "mmn_backproject_nufft_workspace_bytes")
+        if workspace is None or workspace.numel() < nbytes:
+            workspace = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        rc = lib.mmn_backproject_nufft(ctypes.byref(p), _vp(image), _vp(vote), _vp(workspace),
+                                       workspace.numel(), _stream(dev))
+        _lib.check(rc, "mmn_backproject_nufft")
+        return image.view(nx, ny, nz), (vote.view(3, nx, ny, nz) if vote is not None else None)
     nbytes = workspace_bytes(p, mode)
     if workspace is None or workspace.numel() < nbytes:
         workspace = torch.empty(nbytes, dtype=torch.uint8, device=dev)
