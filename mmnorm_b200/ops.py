@@ -295,15 +295,15 @@ class BackprojectFunction(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, meas, pos_offsets, x_locs, y_locs, z_locs, antenna_locs, rx_offsets,
-                wavelength, slope, is_ti_radar):
+                wavelength, slope, is_ti_radar, mode="mixed"):
         image, vote = backproject(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas,
-                                  wavelength, slope, mode="mixed", is_ti_radar=is_ti_radar,
+                                  wavelength, slope, mode=mode, is_ti_radar=is_ti_radar,
                                   pos_offsets=pos_offsets)
         ctx.save_for_backward(meas, pos_offsets, x_locs, y_locs, z_locs, antenna_locs,
                               rx_offsets)
         ctx.consts = (wavelength, slope, is_ti_radar)
         # an output the loss does not use arrives as None, not zeros: without a vote term
-        # the position pass runs one Horner chain instead of two
+        # the passes skip the vote terms
         ctx.set_materialize_grads(False)
         return image, vote
 
@@ -312,24 +312,29 @@ class BackprojectFunction(torch.autograd.Function):
         meas, pos, x, y, z, ant, rxo = ctx.saved_tensors
         wavelength, slope, ti = ctx.consts
         if grad_image is None and grad_vote is None:
-            return (None,) * 10
+            return (None,) * 11
         gm, gp = backproject_backward(
             x, y, z, ant, rxo, meas, wavelength, slope,
             grad_image.contiguous() if grad_image is not None else None,
             grad_vote.contiguous() if grad_vote is not None else None,
             is_ti_radar=ti, pos_offsets=pos, want_meas=ctx.needs_input_grad[0],
             want_pos=ctx.needs_input_grad[1])
-        return gm, gp, None, None, None, None, None, None, None, None
+        return gm, gp, None, None, None, None, None, None, None, None, None
 
 
 def backproject_differentiable(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas,
-                               wavelength, slope, pos_offsets=None, is_ti_radar=False):
-    """(image, vote) with autograd to ``meas`` and ``pos_offsets``."""
+                               wavelength, slope, pos_offsets=None, is_ti_radar=False,
+                               mode="mixed"):
+    """(image, vote) with autograd to ``meas`` and ``pos_offsets``.  ``mode``: "mixed" or
+    "nufft" (the same sums by interpolation; the adjoint's interpolation-form
+    measurement pass is its exact transpose)."""
+    if mode not in ("mixed", "nufft"):
+        raise ValueError("gradients are implemented for mode 'mixed' and 'nufft'")
     if pos_offsets is None:
         pos_offsets = torch.zeros_like(antenna_locs)
     return BackprojectFunction.apply(meas, pos_offsets, x_locs, y_locs, z_locs, antenna_locs,
                                      rx_offsets, float(wavelength), float(slope),
-                                     bool(is_ti_radar))
+                                     bool(is_ti_radar), mode)
 
 
 def normals_differentiable(image, vote, eps=1e-30):

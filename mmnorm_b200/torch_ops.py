@@ -19,7 +19,7 @@ from torch import Tensor
 
 from . import ops
 
-_MODES = ("mixed", "plain", "interp")
+_MODES = ("mixed", "plain", "interp", "nufft")
 
 
 @torch.library.custom_op("mmnorm::backproject", mutates_args=())
@@ -64,8 +64,8 @@ def _(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
 def _setup_context(ctx, inputs, output):
     (x, y, z, ant, rxo, meas, wl, sl, mode, fsp, ti, pos) = inputs
     ctx.set_materialize_grads(False)
-    if mode != "mixed" and (ctx.needs_input_grad[5] or ctx.needs_input_grad[11]):
-        raise NotImplementedError("gradients are implemented for mode='mixed' only")
+    if mode not in ("mixed", "nufft") and (ctx.needs_input_grad[5] or ctx.needs_input_grad[11]):
+        raise NotImplementedError("gradients are implemented for modes 'mixed' and 'nufft'")
     ctx.save_for_backward(x, y, z, ant, rxo, meas, pos)
     ctx.consts = (wl, sl, ti)
 

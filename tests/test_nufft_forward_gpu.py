@@ -71,3 +71,30 @@ def test_sample_count_limit(cuda_dev):
                         _t(sc.z_locs, cuda_dev), _t(sc.antenna_locs, cuda_dev),
                         _t(np.zeros((1, 3), np.float32), cuda_dev), _t(meas, cuda_dev),
                         sc.wavelength, sc.slope, mode="nufft")
+
+
+def test_torch_operator_and_autograd(cuda_dev):
+    """torch.ops.mmnorm.backproject and backproject_differentiable take mode "nufft"; the
+    gradients (the same adjoint kernels) agree with mode "mixed" to the forms' distance."""
+    import torch
+    import mmnorm_b200.torch_ops  # noqa: F401
+    from mmnorm_b200 import ops
+    sc = scenes.sphere_scene(seed=11, n_ap=8, nf=40, n_vox=8, n_pts=20)
+    t = lambda a: _t(a, cuda_dev)
+    args = (t(sc.x_locs), t(sc.y_locs), t(sc.z_locs), t(sc.antenna_locs),
+            t(np.zeros((1, 3), np.float32)))
+    i0, v0 = ops.backproject(*args, t(sc.meas), sc.wavelength, sc.slope, mode="nufft")
+    i1, v1 = torch.ops.mmnorm.backproject(*args, t(sc.meas), sc.wavelength, sc.slope, "nufft",
+                                          0.0, False, None)
+    assert torch.equal(i0, i1) and torch.equal(v0, v1)
+    grads = {}
+    for mode in ("mixed", "nufft"):
+        meas = t(sc.meas).requires_grad_(True)
+        pos = torch.zeros_like(args[3]).requires_grad_(True)
+        img, vote = ops.backproject_differentiable(*args, meas, sc.wavelength, sc.slope,
+                                                   pos_offsets=pos, mode=mode)
+        ((img.abs() ** 2).sum() * 1e-6 + (vote.real ** 2).sum() * 1e-9).backward()
+        grads[mode] = (meas.grad.clone(), pos.grad.clone())
+    rel = lambda a, b: float((a - b).norm() / b.norm())
+    assert rel(grads["nufft"][0], grads["mixed"][0]) < 1e-4
+    assert rel(grads["nufft"][1], grads["mixed"][1]) < 1e-4
