@@ -14,6 +14,12 @@ Two decompositions of the fused backprojection + vote + normal epilogue:
   image and the vote (8 floats per voxel) are all-reduced (SUM) before the epilogue.  For
   grids too small to give every GPU a slab of useful size.
 
+The adjoint (``backproject_backward``, trajectory calibration on several GPUs) splits the
+same ways: with ``"slabs"`` every rank's slab contributes to every measurement and
+antenna-offset gradient, so the partial gradients are all-reduced (SUM) -- the data
+path's one exchange, A (F + 3) values; with ``"antennas"`` a rank owns its antennas' rows
+of both gradients and the rows are all-gathered.
+
 The compute is reached through a backend object (``CudaBackend``: this library's
 kernels).  Every rank issues the same collectives in the same order, including ranks
 whose slab is empty.
@@ -50,6 +56,12 @@ class CudaBackend:
     def normals_from_max(self, image, vote, max_abs, filter_percent):
         from . import ops
         return ops.surface_normals_from_max(image, vote, max_abs, filter_percent)
+
+    def backward(self, x, y, z, ant, rxo, meas, wavelength, slope, grad_image, grad_vote,
+                 **kw):
+        from . import ops
+        return ops.backproject_backward(x, y, z, ant, rxo, meas, wavelength, slope,
+                                        grad_image, grad_vote, **kw)
 
 
 def _world(group):
@@ -144,3 +156,52 @@ def surface_normals(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wave
         x0, x1 = 0, nx
     return {"x_range": (x0, x1), "image": image, "vote": vote, "normals": normals,
             "mask": mask, "max_abs": mx}
+
+
+def backproject_backward(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength,
+                         slope, grad_image, grad_vote, *, decomposition="slabs", group=None,
+                         backend=None, **kw):
+    """Sharded adjoint of the fused backprojection + vote.  Every rank passes the full
+    inputs and the upstream gradients of the WHOLE grid (``grad_image`` complex64
+    [NX, NY, NZ]; ``grad_vote`` [3, NX, NY, NZ] or None) and receives the full gradients
+    ``(grad_meas complex64 [A, F], grad_pos float32 [A, 3])``.  ``kw`` goes to the backend
+    (``is_ti_radar``, ``pos_offsets`` [A, 3])."""
+    be = backend if backend is not None else CudaBackend()
+    world, rank = _world(group)
+    nx = x_locs.numel()
+    A, F = meas.shape
+    R = rx_offsets.shape[0]
+    dev = meas.device
+
+    if decomposition == "slabs":
+        x0, x1 = split_bounds(nx, world, rank)
+        if x1 > x0:
+            gv = grad_vote[:, x0:x1].contiguous() if grad_vote is not None else None
+            gm, gp = be.backward(x_locs[x0:x1].contiguous(), y_locs, z_locs, antenna_locs,
+                                 rx_offsets, meas, wavelength, slope,
+                                 grad_image[x0:x1].contiguous(), gv, **kw)
+        else:
+            gm = torch.zeros((A, F), dtype=torch.complex64, device=dev)
+            gp = torch.zeros((A, 3), dtype=torch.float32, device=dev)
+        if world > 1:
+            _all_reduce(gm, dist.ReduceOp.SUM, group)
+            _all_reduce(gp, dist.ReduceOp.SUM, group)
+        return gm, gp
+    if decomposition == "antennas":
+        a0, a1 = split_bounds(A, world, rank, unit=R)
+        pos = kw.pop("pos_offsets", None)
+        if a1 > a0:
+            gm, gp = be.backward(x_locs, y_locs, z_locs, antenna_locs[a0:a1].contiguous(),
+                                 rx_offsets, meas[a0:a1].contiguous(), wavelength, slope,
+                                 grad_image, grad_vote,
+                                 pos_offsets=None if pos is None else pos[a0:a1].contiguous(),
+                                 **kw)
+        else:
+            gm = torch.zeros((0, F), dtype=torch.complex64, device=dev)
+            gp = torch.zeros((0, 3), dtype=torch.float32, device=dev)
+        if world > 1:
+            counts = [b - a for a, b in (split_bounds(A, world, r, unit=R) for r in range(world))]
+            gm = _gather_slabs(gm, counts, group)
+            gp = _gather_slabs(gp, counts, group)
+        return gm, gp
+    raise ValueError("decomposition must be 'slabs' or 'antennas'")

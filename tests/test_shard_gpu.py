@@ -58,3 +58,24 @@ def test_sharded_single_rank_equals_ops(cuda_dev):
     torch.cuda.synchronize()
     assert torch.equal(res["image"], img) and torch.equal(res["mask"], mask)
     assert torch.equal(torch.nan_to_num(res["normals"], 7.0), torch.nan_to_num(nrm, 7.0))
+
+
+def test_sharded_backward_single_rank_equals_ops(cuda_dev):
+    """One rank: both decompositions of the sharded adjoint are the library's adjoint."""
+    import torch
+    from mmnorm_b200 import ops, shard
+    sc = scenes.sphere_scene(seed=8, n_ap=10, nf=40, n_vox=10, spacing=4e-3, n_pts=30)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=cuda_dev)
+    args = (t(sc.x_locs), t(sc.y_locs), t(sc.z_locs), t(sc.antenna_locs),
+            t(np.zeros((1, 3), np.float32)), t(sc.meas), sc.wavelength, sc.slope)
+    rng = np.random.default_rng(8)
+    V = sc.num_voxels
+    gI = t((rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64))
+    gW = t((rng.standard_normal((3, V)) + 1j * rng.standard_normal((3, V))).astype(np.complex64))
+    shp = (len(sc.x_locs), len(sc.y_locs), len(sc.z_locs))
+    gm, gp = ops.backproject_backward(*args, gI, gW)
+    for dec in ("slabs", "antennas"):
+        gm2, gp2 = shard.backproject_backward(*args, gI.view(shp), gW.view((3,) + shp),
+                                              decomposition=dec)
+        torch.cuda.synchronize()
+        assert torch.equal(gm, gm2) and torch.equal(gp, gp2), dec
