@@ -98,3 +98,33 @@ def test_torch_operator_and_autograd(cuda_dev):
     rel = lambda a, b: float((a - b).norm() / b.norm())
     assert rel(grads["nufft"][0], grads["mixed"][0]) < 1e-4
     assert rel(grads["nufft"][1], grads["mixed"][1]) < 1e-4
+
+
+def test_near_the_sample_limit_forward_and_adjoint(cuda_dev, oracle):
+    """F = 1500: one antenna's grid row (3007 cells, 48 KB) fills a stage on its own, the
+    measurement spread's rows need opt-in shared memory (~113 KB per CTA), and the output
+    transform's 3000-cell grid sits just under 48 KB -- forward and both gradient passes
+    against the oracle."""
+    import torch
+    from mmnorm_b200 import ops
+    nf = 1500
+    sc = scenes.sphere_scene(seed=12, n_ap=4, nf=nf, n_vox=5, n_pts=10)
+    rxo = np.array([[0.0, -0.004, 0.001]], np.float32)
+    I, W = run_ops(cuda_dev, sc, "nufft", rxo=rxo)
+    Io, Wo = oracle.full(sc.voxel_centres(), sc.antenna_locs, rxo, sc.meas, sc.wavelength,
+                         sc.slope)
+    assert oracle.rel_l2(I, Io) < TOL_MIXED and oracle.rel_l2(W, Wo) < TOL_MIXED
+    rng = np.random.default_rng(12)
+    V = sc.num_voxels
+    gI = (rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64)
+    gW = (rng.standard_normal((3, V)) + 1j * rng.standard_normal((3, V))).astype(np.complex64)
+    args = [_t(a, cuda_dev) for a in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs, rxo,
+                                      sc.meas)]
+    gm, gp = ops.backproject_backward(*args, sc.wavelength, sc.slope, _t(gI, cuda_dev),
+                                      _t(gW, cuda_dev))
+    torch.cuda.synchronize()
+    gm_o, gp_o = oracle.full_backward(sc.voxel_centres(), sc.antenna_locs, rxo, sc.meas,
+                                      sc.wavelength, sc.slope, gI.astype(np.complex128),
+                                      gW.T.astype(np.complex128))
+    assert oracle.rel_l2(gm.cpu().numpy().astype(np.complex128), gm_o) < 2e-5
+    assert oracle.rel_l2(gp.cpu().numpy().astype(np.float64), gp_o) < 2e-4
