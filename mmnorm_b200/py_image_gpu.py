@@ -14,7 +14,9 @@ What differs is underneath: one call on the current CUDA device through the sm_1
 library (no per-call JIT, no host threads per GPU, no host-side sum of partial images),
 and the full matched filter runs the mixed-precision kernel (FP64 range and phase
 wrap, FP32 rotation recurrence) instead of one FP64 sin/cos pair per sample.
-``precision='plain'`` selects the FP32 sincos-per-sample kernel instead.
+``precision='plain'`` selects the FP32 sincos-per-sample kernel instead, and
+``precision='nufft'`` the same sums by 8-tap interpolation from per-antenna oversampled
+grids (~2e-6 from the mixed form, faster for F above ~100; F up to ~1500).
 """
 from __future__ import annotations
 
