@@ -37,6 +37,12 @@ def test_image_cuda_full_mode(cuda_dev, oracle, R, use_4_rx, ti):
     assert img.dtype == np.complex64 and img.shape == sc.grid_shape
     assert oracle.rel_l2(img, ref) < 2e-5
     np.testing.assert_array_equal(centres, ref_c)
+    # the same contract with the sums by interpolation (precision="nufft")
+    img_n, centres_n = py_image_gpu.image_cuda(*args, use_4_rx=use_4_rx, is_ti_radar=ti,
+                                               precision="nufft")
+    assert img_n.dtype == np.complex64 and img_n.shape == sc.grid_shape
+    assert oracle.rel_l2(img_n, ref) < 2e-5
+    np.testing.assert_array_equal(centres_n, ref_c)
 
 
 @pytest.mark.parametrize("R,use_4_rx,ti", [(1, False, False), (4, True, True)])
