@@ -105,3 +105,54 @@ def tune_batched(objects, options=(4, 8, 16), repeats=1):
         del plan
     best_ips = min(times, key=times.get)
     return {"best": best_ips, "times_ms": {str(k): v for k, v in times.items()}}
+
+
+def tune_position(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,
+                  grad_image, grad_vote=None, *, max_antennas=1024, repeats=2, apply=True):
+    """Times every launch shape of the interpolation-form position pass (the adjoint's
+    antenna-offset gradient) on a reduced copy of the problem -- the same grid and sample
+    count, at most ``max_antennas`` antennas, the caller's upstream gradients -- and (if
+    ``apply``) selects the fastest.  Cached like ``tune``.
+
+    Returns {"key", "best", "times_ms": {variant index: ms}, "variants": names}."""
+    dev = meas.device
+    nvox = x_locs.numel() * y_locs.numel() * z_locs.numel()
+    key = _key(dev, "position" + ("_vote" if grad_vote is not None else ""), nvox,
+               meas.shape[1])
+    if key in _cache:
+        res = _cache[key]
+        if apply:
+            ops.set_position_variant(res["best"])
+        return res
+    A = meas.shape[0]
+    n = min(A, max_antennas)
+    sel = torch.linspace(0, A - 1, n, device=dev).round().long() if n < A else None
+    ant = antenna_locs[sel].contiguous() if sel is not None else antenna_locs
+    m = meas[sel].contiguous() if sel is not None else meas
+    names = ops.position_variants()
+    stream = torch.cuda.current_stream(dev)
+    times = {}
+
+    def run():
+        ops.backproject_backward(x_locs, y_locs, z_locs, ant, rx_offsets, m, wavelength,
+                                 slope, grad_image, grad_vote, want_meas=False)
+
+    for idx in range(len(names)):
+        ops.set_position_variant(idx)
+        run()
+        best = float("inf")
+        for _ in range(repeats):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            best = min(best, e0.elapsed_time(e1))
+        times[idx] = best
+    best_idx = min(times, key=times.get)
+    res = {"key": key, "best": best_idx, "times_ms": {str(k): t for k, t in times.items()},
+           "variants": names, "antennas_timed": n}
+    _cache[key] = res
+    ops.set_position_variant(best_idx if apply else 0)
+    return res

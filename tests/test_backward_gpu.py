@@ -351,3 +351,29 @@ def test_interpolation_measurement_pass(cuda_dev, oracle, nf, spacing):
     a, b = (out[f].cpu().numpy().astype(np.complex128) for f in ("interp", "horner"))
     assert oracle.rel_l2(b, gm_o) < 2e-5
     assert oracle.rel_l2(a, gm_o) < 2e-5
+
+
+def test_position_autotuner(cuda_dev):
+    """autotune.tune_position times every launch shape, selects the fastest, and the
+    selection gives the gradient of that shape."""
+    import torch
+    from mmnorm_b200 import autotune, ops
+    sc = scenes.sphere_scene(seed=48, n_ap=16, nf=64, n_vox=16, n_pts=20)
+    rng = np.random.default_rng(48)
+    V = sc.num_voxels
+    gI = _t((rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64),
+            cuda_dev)
+    args = [_t(a, cuda_dev) for a in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs,
+                                      np.zeros((1, 3), np.float32), sc.meas)]
+    try:
+        res = autotune.tune_position(*args, sc.wavelength, sc.slope, gI)
+        assert set(res["times_ms"]) == {str(i) for i in range(len(ops.position_variants()))}
+        gp = ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, None,
+                                      want_meas=False)[1]
+        ops.set_position_variant(res["best"])
+        gp2 = ops.backproject_backward(*args, sc.wavelength, sc.slope, gI, None,
+                                       want_meas=False)[1]
+        torch.cuda.synchronize()
+        assert torch.equal(gp, gp2)
+    finally:
+        ops.set_position_variant(0)
