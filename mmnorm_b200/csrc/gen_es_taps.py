@@ -1,7 +1,9 @@
 """Writes es_taps.cuh: the tap weights of the exponential-of-semicircle interpolation kernel
 used by the position pass (bp_nufft.cu), as polynomials in the fractional grid offset.
 
-Kernel: phi(z) = exp(beta (sqrt(1 - (2z/W)^2) - 1)) for |z| < W/2, W = 8, beta = 2.3 W.
+Kernel: phi(z) = exp(beta (sqrt(1 - (2z/W)^2) - 1)) for |z| < W/2, W = 8, beta = 2.3 W --
+the "exponential of semicircle" kernel of Barnett, Magland and af Klinteberg (SIAM J. Sci.
+Comput. 41, 2019) with their width and shape for ~1e-7 at 2x oversampling.
 Tap i (0..7) sits at z = s + W/2 - 1 - i for the fractional offset s in [0, 1).  With
 t = s - 1/2, tap i is P_i(t) = phi(t + W/2 - 1/2 - i) and, phi being even, tap W-1-i is
 P_i(-t).  So only P_0..P_3 are fitted (degree 8, least squares on 4001 points of
