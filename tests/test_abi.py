@@ -53,6 +53,35 @@ def test_version_and_validation_without_device():
     assert h.mmn_num_variants(_lib.MODE_PLAIN) >= 1
 
 
+def test_interpolation_form_and_probe_validation_without_device():
+    """Argument checks of the interpolation-form entry points, the pass selectors and the
+    wait probe, all answered before any device call."""
+    from mmnorm_b200 import _lib
+    h = _lib.load()
+    assert h.mmn_set_position_pass(2) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_set_measurement_pass(-1) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_set_position_pass(0) == _lib.MMN_OK  # the defaults, set again
+    assert h.mmn_set_measurement_pass(0) == _lib.MMN_OK
+    n = h.mmn_num_position_variants()
+    assert n >= 2
+    assert h.mmn_position_variant_name(0).startswith(b"interp_")
+    assert h.mmn_position_variant_name(n) is None
+    assert h.mmn_set_position_variant(n) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_backproject_nufft(None, None, None, None, 0, None) == _lib.MMN_ERR_NULL_POINTER
+    assert h.mmn_backproject_nufft_workspace_bytes(None) == 0
+    p = _lib.MmnProblem()
+    p.num_x = p.num_y = p.num_z = 4
+    p.num_rx = 1
+    p.num_samples = 8
+    p.wavelength = 3.9e-3
+    assert h.mmn_backproject_nufft(ctypes.byref(p), None, None, None, 0, None) == \
+        _lib.MMN_ERR_NULL_POINTER  # no grid axes
+    assert h.mmn_wait_timeout_probe(100, 0, None, None) == _lib.MMN_ERR_NULL_POINTER
+    dummy = ctypes.c_void_p(256)  # never dereferenced: the limit check comes first
+    assert h.mmn_wait_timeout_probe(20000000, 0, dummy, None) == \
+        _lib.MMN_ERR_INVALID_ARGUMENT
+
+
 def test_library_is_sm100a_only_build():
     """The build recipe targets exactly sm_100a."""
     from mmnorm_b200 import build
