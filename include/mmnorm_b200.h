@@ -181,24 +181,38 @@ void mmn_batch_destroy(mmn_batch *batch);
 /*
  * mmn_backproject without any device allocation (no counterpart in the reference, which
  * allocates through pycuda on every call).  For callers that cannot call cudaMalloc
- * where they image -- inside a stream capture, under a host that forbids allocation
- * after start-up, in a real-time loop.  Same inputs, outputs and modes as
- * mmn_backproject; the scratch comes from a 16 MiB device array built into the library,
- * which every GPU that loads the library holds until the process exits.
+ * where they image -- a host that hands its whole device pool to its own allocator and
+ * forbids allocation after start-up, a plugin host that passes only raw device pointers,
+ * a real-time loop that must not block on the allocator.  Same inputs, outputs and modes
+ * as mmn_backproject; the scratch comes from a 16 MiB device array built into the
+ * library, which every GPU (every CUDA context) that loads the library holds until the
+ * process exits.
  *   - Limit: the antenna records plus the staged samples must fit 16 MiB (about
  *     256 + 64*A + 16*A*roundup(F, 32) bytes in the default form, e.g. A*F up to about
  *     one million antenna-samples); larger problems return MMN_ERR_TOO_LARGE before
  *     anything runs.  Every voxel tile takes the whole antenna range (no antenna split),
  *     so problems with few voxels run slower than through mmn_backproject.
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call before any
- *     stream capture.
- *   - All calls share the one array per device and each call re-initialises what it
+ *   - The array's device address belongs to a CUDA context.  The first call in each
+ *     context (normally the device's primary context) looks it up with
+ *     cudaGetSymbolAddress, with that context current, and caches it under the context's
+ *     unique id; make that first call before any stream capture.
+ *   - All calls in a context share the one array and each call re-initialises what it
  *     reads; calls whose work overlaps on the GPU (different streams, or host threads
  *     without ordering) race on it and must be serialised by the caller.
+ *   - The array starts with the status word of its bounded in-kernel waits: read and
+ *     clear it with mmn_noalloc_read_status (MMN_ERR_TIMEOUT there means the last call's
+ *     image and vote are not valid).  The next call clears it.
  */
 int mmn_backproject_noalloc(const mmn_problem *p, int32_t mode, float *image, float *vote,
                             cudaStream_t stream);
+
+/*
+ * Status word of mmn_backproject_noalloc's built-in scratch array in the current context
+ * (mmn_read_status for that array): synchronises `stream`, copies the word to *status and
+ * clears it.  MMN_OK in *status after a completed call; MMN_ERR_TIMEOUT if a bounded wait
+ * gave up.
+ */
+int mmn_noalloc_read_status(int32_t *status, cudaStream_t stream);
 
 /*
  * Unit surface normals from (image, vote): mask |I| > filter_percent * max|I|

@@ -92,6 +92,7 @@ SIGNATURES = [
     ("mmn_plan_info", _I, [_PROB, _I32, _I32P, _I32P, _I32P, _I32P, _I32P]),
     ("mmn_backproject", _I, [_PROB, _I32, _P, _P, _P, _SZ, _P]),
     ("mmn_backproject_noalloc", _I, [_PROB, _I32, _P, _P, _P]),
+    ("mmn_noalloc_read_status", _I, [_I32P, _P]),
     ("mmn_backward_workspace_bytes", _SZ, [_PROB]),
     ("mmn_backproject_nufft_workspace_bytes", _SZ, [_PROB]),
     ("mmn_backproject_nufft", _I, [_PROB, _P, _P, _P, _SZ, _P]),

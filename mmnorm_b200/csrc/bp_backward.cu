@@ -113,7 +113,10 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_kernel(const BwdParams bp) {
     for (int c = 0; c < n_chunks; ++c) {
         const int s = c & 1;
         bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
-        if (!__syncthreads_and(ok)) return;
+        if (!__syncthreads_and(ok)) {
+            st.drain_after_timeout((uint32_t)c, c + 1 < n_chunks, p.status);
+            return;
+        }
         const AntRec *ants = st.ants(s);
         const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
         const int a0 = a_begin + c * st.nas;
@@ -285,7 +288,10 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_img_kernel(const BwdParams bp) 
     for (int c = 0; c < n_chunks; ++c) {
         const int s = c & 1;
         bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
-        if (!__syncthreads_and(ok)) return;
+        if (!__syncthreads_and(ok)) {
+            st.drain_after_timeout((uint32_t)c, c + 1 < n_chunks, p.status);
+            return;
+        }
         const AntRec *ants = st.ants(s);
         const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
         const int a0 = a_begin + c * st.nas;

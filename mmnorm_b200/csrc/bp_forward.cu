@@ -107,7 +107,10 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
         const uint32_t gc = g0 + (uint32_t)c;
         const int s = (int)(gc & 1);
         bool ok = mbar_wait_bounded(&st.bars[s], (gc >> 1) & 1, p.status);
-        if (!__syncthreads_and(ok)) return false;
+        if (!__syncthreads_and(ok)) {
+            st.drain_after_timeout(gc, c + 1 < n_chunks, p.status);
+            return false;
+        }
         const AntRec *ants = st.ants(s);
         const unsigned char *mstage = st.meas(s);
         const int na = min(st.nas, a_end - (a_begin + c * st.nas));

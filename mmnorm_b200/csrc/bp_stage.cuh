@@ -31,6 +31,18 @@ struct Stage {
     __device__ void issue(const FwdParams &p, int c, int a_begin, int a_end) const {
         issue(p, c, c & 1, a_begin, a_end);
     }
+    // Called by every thread after a bounded wait on chunk `gc` gave up (the status word
+    // is set).  The issuing thread gives each stage that may still have a copy outstanding
+    // -- chunk gc, and chunk gc+1 when it was issued -- one more bounded wait, so that a
+    // copy which is merely late lands before the CTA exits and its shared memory can go
+    // to another CTA.  A copy that misses this wait too may still be in flight at exit.
+    __device__ void drain_after_timeout(uint32_t gc, bool next_issued, int32_t *status) const {
+        if (threadIdx.x == 0) {
+            mbar_wait_bounded(&bars[gc & 1], (gc >> 1) & 1, status);
+            if (next_issued) mbar_wait_bounded(&bars[(gc + 1) & 1], ((gc + 1) >> 1) & 1, status);
+        }
+        __syncthreads();
+    }
     __device__ const AntRec *ants(int s) const {
         return reinterpret_cast<const AntRec *>(base + s * stage_bytes);
     }

@@ -15,6 +15,8 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>  // driver types for the context-id lookup (entry points come from the runtime)
+
 #include "bp_kernels.cuh"
 
 using namespace mmn;
@@ -1033,42 +1035,91 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
 // ---------------------------------------------------------------------------------
 // Backprojection that allocates nothing.
 //
-// Some callers cannot call cudaMalloc at the point where they image: code that runs
-// while a stream is being captured, hosts that hand their whole device pool to another
-// allocator and forbid allocation after start-up, and real-time loops that must not
-// block on the allocator.  mmn_backproject_noalloc serves them with a scratch area that
-// is part of the library image itself: a file-scope device array, allocated by the CUDA
-// runtime when the library's module is loaded on a device and held until the process
-// exits.  Its device address is looked up once per device (cudaGetSymbolAddress) on the
-// first call made with that device current.  The caller still owns inputs and outputs.
+// Some callers cannot call cudaMalloc at the point where they image: hosts that hand
+// their whole device pool to another allocator and forbid allocation after start-up,
+// plugin hosts that pass only raw device pointers and own every allocation themselves,
+// and real-time loops that must not block on the allocator.  mmn_backproject_noalloc
+// serves them with a scratch area that is part of the library image itself: a
+// file-scope device array, allocated by the CUDA runtime when the library's module is
+// loaded into a context and held until the process exits.  Its device address is looked
+// up (cudaGetSymbolAddress) on the first call made in each CUDA context, with that
+// context current, and cached under the context's unique id -- an address from one
+// context is not mapped in another, and a context created after cudaDeviceReset gets a
+// new id.  The caller still owns inputs and outputs.
 // ---------------------------------------------------------------------------------
 namespace {
 
-constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;  // 16 MiB per device
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;  // 16 MiB per context
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void *g_noalloc_addr[kNoAllocMaxDevices] = {};
+typedef CUresult(CUDAAPI *CtxGetCurrentFn)(CUcontext *);
+typedef CUresult(CUDAAPI *CtxGetIdFn)(CUcontext, unsigned long long *);
 
-// Device address of the scratch array on the current device.  In host code the array's
+struct NoAllocEntry {
+    unsigned long long ctx_id;
+    void *addr;
+};
+std::mutex g_noalloc_mutex;
+std::vector<NoAllocEntry> g_noalloc_cache;
+bool g_noalloc_fns_looked_up = false;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// Unique id of the calling thread's current context; false when no context is current
+// or the driver cannot tell (then nothing is cached).  Caller holds g_noalloc_mutex.
+bool current_context_id(unsigned long long *id) {
+    if (!g_noalloc_fns_looked_up) {
+        g_noalloc_fns_looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent",
+                                             reinterpret_cast<void **>(&g_ctx_get_current),
+                                             12000, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess)
+            g_ctx_get_current = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId",
+                                             reinterpret_cast<void **>(&g_ctx_get_id), 12000,
+                                             cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            g_ctx_get_id = nullptr;
+        cudaGetLastError();  // a failed lookup leaves nothing behind for later calls
+    }
+    if (!g_ctx_get_current || !g_ctx_get_id) return false;
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return g_ctx_get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of the scratch array in the current context.  In host code the array's
 // name only stands in for the symbol, so the address has to come from the runtime.
 int noalloc_scratch(void **out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return MMN_ERR_CUDA;
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return MMN_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-        void *addr = nullptr;
-        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr)
-            return MMN_ERR_CUDA;
-        g_noalloc_addr[dev] = addr;
+    unsigned long long id = 0;
+    if (current_context_id(&id)) {
+        for (const NoAllocEntry &e : g_noalloc_cache)
+            if (e.ctx_id == id) {
+                *out = e.addr;
+                return MMN_OK;
+            }
     }
-    *out = g_noalloc_addr[dev];
+    // first call in this context (cudaGetSymbolAddress also makes the device's primary
+    // context current if no context is)
+    void *addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr)
+        return MMN_ERR_CUDA;
+    if (current_context_id(&id)) g_noalloc_cache.push_back({id, addr});
+    *out = addr;
     return MMN_OK;
 }
 
 }  // namespace
+
+extern "C" int mmn_noalloc_read_status(int32_t *status, cudaStream_t stream) {
+    if (!status) return MMN_ERR_NULL_POINTER;
+    void *scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc != MMN_OK) return rc;
+    return mmn_read_status(scratch, status, stream);
+}
 
 extern "C" int mmn_backproject_noalloc(const mmn_problem *p, int32_t mode, float *image,
                                        float *vote, cudaStream_t stream) {

@@ -48,6 +48,8 @@ def test_version_and_validation_without_device():
         _lib.MMN_ERR_NULL_POINTER
     assert h.mmn_normals(0, None, None, 0.05, None, None, None, None, 0, None) == \
         _lib.MMN_ERR_INVALID_ARGUMENT
+    # the no-alloc status accessor checks its output pointer before touching a device
+    assert h.mmn_noalloc_read_status(None, None) == _lib.MMN_ERR_NULL_POINTER
     assert h.mmn_set_variant(7, 0) == _lib.MMN_ERR_INVALID_ARGUMENT
     assert h.mmn_num_variants(_lib.MODE_MIXED) >= 1
     assert h.mmn_num_variants(_lib.MODE_PLAIN) >= 1

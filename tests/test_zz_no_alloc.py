@@ -94,3 +94,38 @@ def test_noalloc_rejects_problems_beyond_its_scratch(cuda_dev):
     args = _tensors(cuda_dev, sc, meas=meas, ant=ant)
     rc, _, _ = _noalloc(args, sc, "mixed", cuda_dev)
     assert rc == _lib.MMN_ERR_TOO_LARGE
+
+
+def test_noalloc_status_word_reads_ok_after_a_call(cuda_dev):
+    import torch
+    from mmnorm_b200 import _lib, ops
+    sc = scenes.sphere_scene(seed=33, n_ap=8, nf=32, n_vox=8, n_pts=20)
+    args = _tensors(cuda_dev, sc)
+    rc, _, _ = _noalloc(args, sc, "mixed", cuda_dev)
+    assert rc == _lib.MMN_OK
+    status = ctypes.c_int32(-1)
+    assert _lib.load().mmn_noalloc_read_status(ctypes.byref(status),
+                                               ops._stream(cuda_dev)) == _lib.MMN_OK
+    assert status.value == _lib.MMN_OK
+    torch.cuda.synchronize()
+
+
+def test_noalloc_just_under_its_scratch_limit(cuda_dev):
+    """4000 antennas x 256 samples: 256 + 64*4000 + 16*4000*256 bytes of records and
+    staged samples: 16,640,256 of the array's 16,777,216 bytes."""
+    import torch
+    from mmnorm_b200 import _lib, ops
+    sc = scenes.sphere_scene(seed=34, n_ap=4, nf=256, n_vox=8, n_pts=20)
+    A, F = 4000, 256
+    rng = np.random.default_rng(34)
+    meas = (rng.standard_normal((A, F)) + 1j * rng.standard_normal((A, F))).astype(np.complex64)
+    g = np.arange(A)
+    ant = np.stack([(g % 80 - 40) * 2e-3, (g // 80 - 25) * 2e-3, np.zeros(A)], 1)
+    args = _tensors(cuda_dev, sc, meas=meas, ant=ant.astype(np.float32))
+    ref_img, ref_vote = ops.backproject(*args, sc.wavelength, sc.slope, mode="mixed")
+    for _ in range(2):
+        rc, img, vote = _noalloc(args, sc, "mixed", cuda_dev)
+        assert rc == _lib.MMN_OK
+        torch.cuda.synchronize()
+        assert _rel(img, ref_img) < TOL
+        assert _rel(vote, ref_vote) < TOL
