@@ -50,6 +50,12 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-interp", action="store_true",
+                    help="skip the interpolated-mode leg (reference kernels, bit-exact and "
+                         "fast forms)")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the reference CUDA kernel's full matched filter")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--variant", default=None,
                     help="force a mixed kernel variant by name instead of autotuning")
     ap.add_argument("--aperture", type=int, default=128,
@@ -331,6 +337,21 @@ def ours_arm(args):
     value = world * updates * args.steps / (total_ms * 1e-3) / 1e9
     kern_ms = [a.elapsed_time(b) for a, b in kernel_events]
     kern_avg_s = statistics.mean(kern_ms) * 1e-3
+
+    # outputs on a seeded 4096-voxel subset, for the accuracy report against the FP64 oracle
+    acc_idx = np.sort(np.random.default_rng(2).choice(V, 4096, replace=False))
+    acc_t = torch.as_tensor(acc_idx, device=dev)
+
+    def subset(img, vote):
+        I = img.reshape(-1)[acc_t].cpu().numpy()
+        W = vote.reshape(3, -1)[:, acc_t].cpu().numpy().T
+        return (I, W), float(img.abs().max())
+
+    acc_mixed = acc_plain = None
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        img_a, vote_a, _, _ = step()
+        acc_mixed = subset(img_a, vote_a)
+        del img_a, vote_a
     # prep_antennas, stage_meas, bp_fwd_kernel (+ bp_reduce_partials), max_abs, normals
     launches_per_step = 5 + (1 if plan["splits"] > 1 else 0)
 
@@ -351,6 +372,10 @@ def ours_arm(args):
         torch.cuda.synchronize()
         pms = p0.elapsed_time(p1) / args.plain_steps
         pval = updates / (pms * 1e-3) / 1e9
+        if not args.no_accuracy:
+            img_a, vote_a, _, _ = step("plain")
+            acc_plain = subset(img_a, vote_a)
+            del img_a, vote_a
         out["plain"] = {"value": pval, "unit": UNIT, "ms_per_step": pms,
                         "kernel_ms": statistics.mean(a.elapsed_time(b) for a, b in pe),
                         "mixed_over_plain": value / pval,
@@ -466,6 +491,18 @@ def ours_arm(args):
                               "semantics): numpy inputs -> complex64 image, float64 unit "
                               "normals with NaN, phase centres; wall clock, one call"}
 
+    interp = None
+    if rank == 0 and world == 1 and not args.no_interp and args.aperture == 128:
+        interp = time_interp(dev, sc)
+    reference_cuda = None
+    if rank == 0 and world == 1 and not args.no_reference_cuda and args.aperture == 128:
+        reference_cuda = time_reference_cuda_full(dev, sc)
+    accuracy = None
+    if acc_mixed is not None:
+        accuracy = accuracy_report(dev, sc, acc_idx, acc_mixed[0],
+                                   acc_plain[0] if acc_plain else None, acc_mixed[1],
+                                   acc_plain[1] if acc_plain else None)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -541,7 +578,7 @@ def ours_arm(args):
                        "autotune_ms": tuned["times_ms"]},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": _read_traffic(),
+                         "traffic": FWD_DRAM_BYTES_PER_LAUNCH,
                          "kernel": "bp_fwd_kernel " + variant["name"],
                          "flops_per_update": 8,
                          "peak_source": "FP32 FFMA probe (mmn_fp32_peak_probe) timed in this "
@@ -560,6 +597,9 @@ def ours_arm(args):
             "numpy_baseline": numpy_cpu,
             "adjoint": adjoint,
             "batched": batched,
+            "interp": interp,
+            "reference_cuda": reference_cuda,
+            "accuracy": accuracy,
         }
         line.update(out)
         print(json.dumps(line))
@@ -679,19 +719,333 @@ def time_batched(dev, replays=3):
             "graph": "captured once, replayed"}
 
 
-def _read_traffic():
-    """DRAM bytes per launch of the forward kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "bp_fwd_mixed_boxcyl128.md")
-    if not os.path.exists(path):
-        return None
-    with open(path) as f:
-        for line in f:
-            if line.startswith("dram_bytes_per_launch_full_size:"):
-                try:
-                    return float(line.split(":", 1)[1].split()[0])
-                except ValueError:
-                    return None
-    return None
+def _event_ms(fn, reps=3, warm=1):
+    """CUDA-event times (ms) of `fn` on the current stream: `warm` untimed calls, then
+    `reps` timed ones; returns the list."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def _wall_ms(fn, reps=2, warm=1):
+    """Host wall-clock times (ms) of a synchronous call, synchronised on both sides."""
+    import torch
+    for _ in range(warm):
+        fn()
+    out = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        out.append(1e3 * (time.perf_counter() - t0))
+    return out
+
+
+def _central_antennas(n_side, full_side=128):
+    n0 = (full_side - n_side) // 2
+    return (np.arange(n0, n0 + n_side)[:, None] * full_side +
+            np.arange(n0, n0 + n_side)[None, :]).ravel()
+
+
+def time_reference_cuda_full(dev, sc, target_ms=1000.0):
+    """The reference's own CUDA kernel (cuda_image, full matched filter: FP32 range, FP64
+    phase and FP64 sin + cos per update, imaging_gpu.cu:106-117), compiled unmodified for
+    sm_100a and launched as py_image_gpu.py:272-274 does (block 512, grid V/512 + 1), on the
+    WHOLE 128^3 grid -- so it fills the GPU as it would in use -- with a central n x n
+    subset of the aperture sized so that one reference launch takes about `target_ms`.
+    mmn_cuda_image (the drop-in entry with the reference's argument list, mixed form) runs
+    on the same inputs.  Kernel-only CUDA-event times, and end to end: the reference with
+    its per-call pycuda transfers (allocation + synchronous copies from pageable memory,
+    oracle/ref_cuda.cuda_image_in_out), ours through mmn_cuda_image from the same pageable
+    arrays."""
+    import torch
+    from mmnorm_b200 import _lib, ops
+    from oracle import ref_cuda
+    if not ref_cuda.available():
+        return {"unavailable": "reference cubins not built (oracle/build.py needs the mmNorm "
+                               "checkout at build time)"}
+    nx, ny, nz = sc.grid_shape
+    V = nx * ny * nz
+    F = sc.meas.shape[1]
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    x, y, z = t(sc.x_locs), t(sc.y_locs), t(sc.z_locs)
+    rxo = t(np.zeros(3, np.float32))
+    wl, sl = np.float32(sc.wavelength), np.float32(sc.slope)
+    lib = _lib.load()
+    vp = ops._vp
+
+    def inputs(n_side):
+        idx = _central_antennas(n_side)
+        ant = np.ascontiguousarray(sc.antenna_locs[idx])
+        m = sc.meas[idx]
+        return (idx.size, ant, np.ascontiguousarray(m.real.reshape(-1)),
+                np.ascontiguousarray(m.imag.reshape(-1)))
+
+    def ref_kernel_ms(n_side, reps):
+        A, ant, mr, mi = inputs(n_side)
+        pr, pi = torch.zeros(V, device=dev), torch.zeros(V, device=dev)
+        ta, tr, ti_ = t(ant.reshape(-1)), t(mr), t(mi)
+        ms = _event_ms(lambda: ref_cuda.cuda_image(pr, pi, x, y, z, ta, tr, ti_, rxo, sl, wl,
+                                                   0.0, nx, ny, nz, A, 1, F, 0, 0),
+                       reps=reps, warm=0 if reps == 1 else 1)
+        return ms, (pr, pi)
+
+    # calibrate on 4 x 4 antennas, then size the subset for ~target_ms per launch
+    cal, _ = ref_kernel_ms(4, 1)
+    n_side = int(max(4, min(128, math.floor(math.sqrt(16 * target_ms / max(cal[0], 1e-3))))))
+    A, ant, mr, mi = inputs(n_side)
+    ref_ms, (pr, pi) = ref_kernel_ms(n_side, 2)
+    ta, tr, ti_ = t(ant.reshape(-1)), t(mr), t(mi)
+    ws_n = lib.mmn_cuda_image_workspace_bytes_for(nx, ny, nz, A, F, 0, -1, 0)
+    ws = torch.empty(ws_n, dtype=torch.uint8, device=dev)
+    qr, qi = torch.zeros(V, device=dev), torch.zeros(V, device=dev)
+
+    def ours():
+        _lib.check(lib.mmn_cuda_image(vp(qr), vp(qi), vp(x), vp(y), vp(z), vp(ta), vp(tr),
+                                      vp(ti_), vp(rxo), float(sl), float(wl), 0.0, nx, ny, nz,
+                                      A, 1, F, 0, 0, 0, -1, vp(ws), ws_n, ops._stream(dev)),
+                   "mmn_cuda_image")
+
+    ours_ms = _event_ms(ours, reps=3)
+    upd = V * A * F
+    a = pr.cpu().numpy().astype(np.float64) + 1j * pi.cpu().numpy()
+    b = qr.cpu().numpy().astype(np.float64) + 1j * qi.cpu().numpy()
+    rel = float(np.linalg.norm(a - b) / np.linalg.norm(a))
+    # end to end, host numpy in and out every call
+    hx, hy, hz = sc.x_locs, sc.y_locs, sc.z_locs
+    hant, hrxo = ant.reshape(-1), np.zeros(3, np.float32)
+    ref_e2e = _wall_ms(lambda: ref_cuda.cuda_image_in_out(hx, hy, hz, hant, mr, mi, hrxo, sl, wl,
+                                                          0.0, A, 1, F, 0, 0), reps=1, warm=0)
+    out_r, out_i = np.empty(V, np.float32), np.empty(V, np.float32)
+
+    def ours_e2e():
+        dx, dy, dz, da, dr, di, do = (torch.from_numpy(np.asarray(h)).to(dev)
+                                      for h in (hx, hy, hz, hant, mr, mi, hrxo))
+        ox, oi = torch.empty(V, device=dev), torch.empty(V, device=dev)
+        w = torch.empty(ws_n, dtype=torch.uint8, device=dev)
+        _lib.check(lib.mmn_cuda_image(vp(ox), vp(oi), vp(dx), vp(dy), vp(dz), vp(da), vp(dr),
+                                      vp(di), vp(do), float(sl), float(wl), 0.0, nx, ny, nz, A,
+                                      1, F, 0, 0, 0, -1, vp(w), ws_n, ops._stream(dev)),
+                   "mmn_cuda_image")
+        out_r[:] = ox.cpu().numpy()
+        out_i[:] = oi.cpu().numpy()
+
+    ours_e2e_ms = _wall_ms(ours_e2e, reps=3)
+    r_ms, o_ms = min(ref_ms), min(ours_ms)
+    re_ms, oe_ms = min(ref_e2e), min(ours_e2e_ms)
+    return {
+        "what": "reference cuda_image full matched filter vs mmn_cuda_image (mixed) on the "
+                "whole 128^3 grid with the central %dx%d antennas x %d freqs" % (n_side, n_side, F),
+        "antennas": A, "updates": upd, "launch": "reference: block 512, grid %d" % (V // 512 + 1),
+        "reference_kernel_ms": r_ms, "reference_G_updates_per_s": upd / r_ms / 1e6,
+        "ours_kernel_ms": o_ms, "ours_G_updates_per_s": upd / o_ms / 1e6,
+        "kernel_speedup": r_ms / o_ms,
+        "reference_e2e_ms": re_ms, "reference_e2e_G_updates_per_s": upd / re_ms / 1e6,
+        "ours_e2e_ms": oe_ms, "ours_e2e_G_updates_per_s": upd / oe_ms / 1e6,
+        "e2e_speedup": re_ms / oe_ms,
+        "e2e_path": "reference: pycuda drv.In/Out pattern (cuMemAlloc + synchronous copies from "
+                    "pageable numpy, launch, copy back, free); ours: mmn_cuda_image with torch "
+                    "device buffers from the same pageable arrays; host wall clock",
+        "rel_l2_ours_vs_reference": rel}
+
+
+def time_interp(dev, sc, nbins=4096):
+    """Interpolated mode, the reference's shipped default (src/utils/params.json:4), on the
+    whole workload: the 256-sample measurements zero-padded to a 4096-bin range FFT
+    (image_processor.py:22-35, here torch.fft on the device), 2.1M voxels x 16384 antennas.
+    The reference's own cuda_image (interpolated branch) and cuda_sn_est against this
+    library's bit-exact kernels and the fast form, kernel-only CUDA events; the fast form
+    also fused with the vote in one pass; end to end with the reference's per-call pycuda
+    transfers vs ours from the same pageable arrays."""
+    import torch
+    from mmnorm_b200 import _lib, ops
+    from oracle import ref_cuda
+    nx, ny, nz = sc.grid_shape
+    V = nx * ny * nz
+    A, F = sc.meas.shape
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    x, y, z = t(sc.x_locs), t(sc.y_locs), t(sc.z_locs)
+    ant = t(sc.antenna_locs)
+    rxo = t(np.zeros((1, 3), np.float32))
+    pad = torch.zeros((A, nbins), dtype=torch.complex64, device=dev)
+    pad[:, :F] = t(sc.meas)
+    fft = torch.fft.fft(pad, dim=1)
+    del pad
+    mr, mi = fft.real.contiguous().reshape(-1), fft.imag.contiguous().reshape(-1)
+    fsp = np.float32(3e8 / (2 * (sc.f_hi - sc.f_lo)) * F / nbins)
+    wl, sl = np.float32(sc.wavelength), np.float32(sc.slope)
+    lib = _lib.load()
+    vp = ops._vp
+    ws = torch.empty(256, dtype=torch.uint8, device=dev)
+    qr, qi = torch.zeros(V, device=dev), torch.zeros(V, device=dev)
+
+    def ours(flag, out_r=qr, out_i=qi):
+        _lib.check(lib.mmn_cuda_image(vp(out_r), vp(out_i), vp(x), vp(y), vp(z), vp(ant),
+                                      vp(mr), vp(mi), vp(rxo), float(sl), float(wl), float(fsp),
+                                      nx, ny, nz, A, 1, nbins, 0, 0, flag, -1, vp(ws), 256,
+                                      ops._stream(dev)),
+                   "mmn_cuda_image")
+
+    pairs = V * A
+    out = {"what": "interpolated mode, 128^3 voxels x 16384 antennas, %d-bin range FFT" % nbins,
+           "pairs": pairs}
+    exact_ms = _event_ms(lambda: ours(1))
+    exact = torch.complex(qr, qi).clone()
+    fast_ms = _event_ms(lambda: ours(2))
+    fast = torch.complex(qr, qi).clone()
+    rel = lambda a, b: float((a.to(torch.complex128) - b.to(torch.complex128)).norm() /
+                             b.to(torch.complex128).norm())
+    out["ours_exact_ms"] = min(exact_ms)
+    out["ours_fast_ms"] = min(fast_ms)
+    out["fast_rel_l2_vs_exact"] = rel(fast, exact)
+    img_f, vote_f = ops.backproject(x, y, z, ant, rxo, fft, float(wl), float(sl),
+                                    mode="interp_fast", fft_spacing=float(fsp))
+    fused_ms = _event_ms(lambda: ops.backproject(x, y, z, ant, rxo, fft, float(wl), float(sl),
+                                                 mode="interp_fast", fft_spacing=float(fsp)))
+    out["ours_fast_fused_image_vote_ms"] = min(fused_ms)
+    del img_f, vote_f
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    # 3 MUFU results per pair (square-root seed, sine, cosine) at 16 per SM per clock
+    out["fast_mufu_bound"] = {"mufu_per_pair": 3, "sm_count": sms,
+                              "bound_pairs_per_s_at_1965MHz": sms * 16 / 3 * 1.965e9,
+                              "frac": pairs / (min(fast_ms) * 1e-3) / (sms * 16 / 3 * 1.965e9)}
+    if ref_cuda.available():
+        pr, pi = torch.zeros(V, device=dev), torch.zeros(V, device=dev)
+        ref_ms = _event_ms(lambda: ref_cuda.cuda_image(pr, pi, x, y, z, ant.reshape(-1), mr, mi,
+                                                       rxo.reshape(-1), sl, wl, fsp, nx, ny, nz,
+                                                       A, 1, nbins, 0, 1))
+        torch.cuda.synchronize()
+        out["reference_kernel_ms"] = min(ref_ms)
+        out["exact_bit_identical_to_reference"] = bool(torch.equal(pr, exact.real) and
+                                                       torch.equal(pi, exact.imag))
+        out["exact_speedup"] = min(ref_ms) / min(exact_ms)
+        out["fast_speedup"] = min(ref_ms) / min(fast_ms)
+        out["fast_rel_l2_vs_reference"] = rel(fast, torch.complex(pr, pi))
+        # normal vote over the masked voxels (py_sn_est_gpu.py:326-333)
+        img = torch.complex(pr, pi).reshape(nx, ny, nz)
+        mag = img.abs()
+        coords = torch.nonzero(mag > mag.max() * 0.05).to(torch.int32)
+        nv = int(coords.shape[0])
+        vx, vy, vz = (coords[:, k].contiguous() for k in range(3))
+        out["normals"] = {"valid_voxels": nv}
+        outs = {}
+        for which in ("reference", "exact", "fast"):
+            n = [torch.zeros(nv, device=dev) for _ in range(3)]
+            if which == "reference":
+                fn = lambda n=n: ref_cuda.cuda_sn_est(*n, vx, vy, vz, pr, pi, x, y, z,
+                                                      ant.reshape(-1), mr, mi, rxo.reshape(-1),
+                                                      sl, wl, fsp, nx, ny, nz, A, 1, nv, nbins,
+                                                      0)
+            else:
+                entry = lib.mmn_cuda_sn_est if which == "exact" else lib.mmn_cuda_sn_est_fast
+                fn = lambda n=n, entry=entry: _lib.check(entry(
+                    vp(n[0]), vp(n[1]), vp(n[2]), vp(vx), vp(vy), vp(vz), vp(pr), vp(pi), vp(x),
+                    vp(y), vp(z), vp(ant), vp(mr), vp(mi), vp(rxo), float(sl), float(wl),
+                    float(fsp), nx, ny, nz, A, 1, nv, nbins, 0, 0, -1, vp(ws), 256,
+                    ops._stream(dev)), "mmn_cuda_sn_est")
+            out["normals"][which + "_ms"] = min(_event_ms(fn))
+            outs[which] = torch.stack(n, 1)
+        out["normals"]["exact_bit_identical_to_reference"] = bool(
+            torch.equal(outs["exact"], outs["reference"]))
+        out["normals"]["fast_rel_l2_vs_reference"] = rel(outs["fast"], outs["reference"])
+        out["normals"]["fast_speedup"] = out["normals"]["reference_ms"] / out["normals"]["fast_ms"]
+        # end to end (image), host numpy in and out every call
+        hx, hy, hz = sc.x_locs, sc.y_locs, sc.z_locs
+        hant = np.ascontiguousarray(sc.antenna_locs.reshape(-1))
+        hmr, hmi = mr.cpu().numpy(), mi.cpu().numpy()
+        hrxo = np.zeros(3, np.float32)
+        ref_e2e = _wall_ms(lambda: ref_cuda.cuda_image_in_out(hx, hy, hz, hant, hmr, hmi, hrxo, sl,
+                                                              wl, fsp, A, 1, nbins, 0, 1))
+        o_r, o_i = np.empty(V, np.float32), np.empty(V, np.float32)
+
+        def ours_e2e(flag):
+            dx, dy, dz, da, dr, di, do = (torch.from_numpy(np.asarray(h)).to(dev)
+                                          for h in (hx, hy, hz, hant, hmr, hmi, hrxo))
+            ox, oi = torch.empty(V, device=dev), torch.empty(V, device=dev)
+            _lib.check(lib.mmn_cuda_image(vp(ox), vp(oi), vp(dx), vp(dy), vp(dz), vp(da),
+                                          vp(dr), vp(di), vp(do), float(sl), float(wl),
+                                          float(fsp), nx, ny, nz, A, 1, nbins, 0, 0, flag, -1,
+                                          vp(ws), 256, ops._stream(dev)), "mmn_cuda_image")
+            o_r[:] = ox.cpu().numpy()
+            o_i[:] = oi.cpu().numpy()
+
+        out["e2e"] = {"reference_ms": min(ref_e2e),
+                      "ours_exact_ms": min(_wall_ms(lambda: ours_e2e(1))),
+                      "ours_fast_ms": min(_wall_ms(lambda: ours_e2e(2))),
+                      "h2d_bytes": int(hmr.nbytes + hmi.nbytes + hant.nbytes + 4 * (nx + ny + nz)),
+                      "d2h_bytes": 8 * V,
+                      "path": "reference: pycuda drv.In/Out pattern; ours: mmn_cuda_image from "
+                              "the same pageable arrays; host wall clock"}
+        out["e2e"]["fast_speedup"] = out["e2e"]["reference_ms"] / out["e2e"]["ours_fast_ms"]
+    else:
+        out["reference"] = "unavailable: reference cubins not built"
+    return out
+
+
+def accuracy_report(dev, sc, idx, sub_mixed, sub_plain, max_mixed, max_plain):
+    """Relative L2 error of the complex image and the vote, and the median / 95th
+    percentile normal angle over the masked voxels, of the mixed and plain forms against
+    the FP64 oracle: the workload on a seeded random 4096-voxel subset (from the step's own
+    outputs), and config 2 (the 48^3 sphere scene of config 0, 32x32 antennas, 64
+    frequencies) on its seeded 4096-voxel subset."""
+    import torch
+    from mmnorm_b200 import ops, scenes
+    from oracle import oracle as O
+
+    def stats(I, W, Io, Wo, max_full):
+        sel = np.abs(Io) > 0.05 * max_full
+        _, _, raw_o = O.normals_from_vote(Io, Wo, 0.0)
+        _, _, raw = O.normals_from_vote(I.astype(np.complex128), W.astype(np.complex128), 0.0)
+        ang = O.angle_deg(raw[sel], raw_o[sel])
+        return {"image_rel_l2": O.rel_l2(I, Io), "vote_rel_l2": O.rel_l2(W, Wo),
+                "normal_deg_median": float(np.median(ang)) if ang.size else None,
+                "normal_deg_p95": float(np.percentile(ang, 95)) if ang.size else None,
+                "masked_voxels": int(sel.sum())}
+
+    rxo = np.zeros((1, 3))
+    t0 = time.perf_counter()
+    Io, Wo = O.full(sc.voxel_centres(idx), sc.antenna_locs, rxo, sc.meas, sc.wavelength,
+                    sc.slope, phase_mode=1)
+    out = {"workload_subset": {"voxels": int(len(idx)), "sign": -1,
+                               "mixed": stats(*sub_mixed, Io, Wo, max_mixed)}}
+    if sub_plain is not None:
+        out["workload_subset"]["plain"] = stats(*sub_plain, Io, Wo, max_plain)
+    sc2 = scenes.config0(sign=-1)
+    idx2 = np.sort(np.random.default_rng(2).choice(sc2.num_voxels, 4096, replace=False))
+    Io2, Wo2 = O.full(sc2.voxel_centres(idx2), sc2.antenna_locs, rxo, sc2.meas, sc2.wavelength,
+                      sc2.slope, phase_mode=1)
+    tt = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    out["config2"] = {"scene": sc2.name, "voxels": 4096}
+    for mode in ("mixed", "plain"):
+        img, vote = ops.backproject(tt(sc2.x_locs), tt(sc2.y_locs), tt(sc2.z_locs),
+                                    tt(sc2.antenna_locs), tt(np.zeros((1, 3), np.float32)),
+                                    tt(sc2.meas), sc2.wavelength, sc2.slope, mode=mode)
+        I = img.cpu().numpy().ravel()
+        W = vote.cpu().numpy().reshape(3, -1).T
+        out["config2"][mode] = stats(I[idx2], W[idx2], Io2, Wo2, float(np.abs(I).max()))
+    out["oracle"] = "FP64 C restatement (oracle/bp_oracle.c) on float32-rounded inputs"
+    out["oracle_seconds"] = time.perf_counter() - t0
+    return out
+
+
+
+# DRAM bytes (read + write) of one forward launch at the workload, from one ncu capture of
+# the central 32x32-antenna case (dram__bytes_read.sum + dram__bytes_write.sum of
+# bp_fwd_kernel, -c 1) scaled by the antenna count (x16): the staged rows are re-read per
+# CTA, so the traffic grows with the antennas a CTA sweeps.  Capture and scaling are
+# summarised in profiles/bp_fwd_kernel_boxcyl128_ap32.md.
+FWD_DRAM_BYTES_PER_LAUNCH = None
 
 
 def main():

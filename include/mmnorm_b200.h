@@ -44,6 +44,12 @@ extern "C" {
 #define MMN_MODE_MIXED 0  /* FP64 range + wrap, FP32 rotation recurrence (default)  */
 #define MMN_MODE_PLAIN 1  /* FP32 range and phase, one sincosf per sample           */
 #define MMN_MODE_INTERP 2 /* reference interpolated mode (range-FFT bin + 1 phasor) */
+/* Interpolated mode, fast form (no counterpart in the reference): the reference's FP32
+ * path length and range bin, so the same range-FFT sample is gathered, with the phasor
+ * exp(-j 2 pi d / lambda) formed from the wrapped FP32 turn count (1/lambda split into two
+ * floats) and the hardware sine/cosine instead of FP64 cos and sin: about 5e-7 relative
+ * per term from the reference's phasor.  Bins up to 2^22 (else MMN_ERR_TOO_LARGE). */
+#define MMN_MODE_INTERP_FAST 3
 
 /* Problem description.  All array pointers are device pointers. */
 typedef struct mmn_problem {
@@ -352,7 +358,8 @@ int mmn_correlate_poses(const double *times, const double *traj, int64_t num_poi
  * threads_per_block, py_image_gpu.py:273,187; -1 = to the end of the grid), a
  * workspace and a stream.  Writes p_xyz_r/p_xyz_i for voxels [start_ind,
  * start_ind + voxel_count).  use_interpolated_processing == 0 runs the mixed-precision
- * matched filter; != 0 runs the interpolated mode with the reference's arithmetic.
+ * matched filter; 1 runs the interpolated mode with the reference's arithmetic (bit for
+ * bit); 2 runs the interpolated mode's fast form (MMN_MODE_INTERP_FAST).
  */
 size_t mmn_cuda_image_workspace_bytes(int num_antennas, int samples_per_meas,
                                       int use_interpolated_processing);
@@ -388,6 +395,23 @@ int mmn_cuda_sn_est(float *normals_x, float *normals_y, float *normals_z,
                     int num_antennas, int num_rx_antennas, int num_valid_idx,
                     int samples_per_meas, int start_ind, int is_ti_radar, int count,
                     void *workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/*
+ * mmn_cuda_sn_est in the fast form of MMN_MODE_INTERP_FAST (no counterpart in the
+ * reference): same arguments, valid-voxel list and outputs; the reference's path length
+ * and range bin, the phasor from the wrapped FP32 turn count and the hardware
+ * sine/cosine, and the weight as one multiply by 1/|I|.
+ */
+int mmn_cuda_sn_est_fast(float *normals_x, float *normals_y, float *normals_z,
+                         const int *valid_idx_x, const int *valid_idx_y,
+                         const int *valid_idx_z, const float *p_xyz_r, const float *p_xyz_i,
+                         const float *x_locs, const float *y_locs, const float *z_locs,
+                         const float *antenna_locs, const float *meas_r, const float *meas_i,
+                         const float *rx_offsets, float slope, float wavelength,
+                         float fft_spacing, int num_x, int num_y, int num_z,
+                         int num_antennas, int num_rx_antennas, int num_valid_idx,
+                         int samples_per_meas, int start_ind, int is_ti_radar, int count,
+                         void *workspace, size_t workspace_bytes, cudaStream_t stream);
 
 /*
  * FP32 FMA throughput probe (no counterpart in the reference): `blocks` CTAs of 256

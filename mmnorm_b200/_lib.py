@@ -23,7 +23,9 @@ MMN_ERR_TOO_LARGE = 7
 MODE_MIXED = 0
 MODE_PLAIN = 1
 MODE_INTERP = 2
-MODES = {"mixed": MODE_MIXED, "plain": MODE_PLAIN, "interp": MODE_INTERP}
+MODE_INTERP_FAST = 3
+MODES = {"mixed": MODE_MIXED, "plain": MODE_PLAIN, "interp": MODE_INTERP,
+         "interp_fast": MODE_INTERP_FAST}
 
 _ERR_NAMES = {
     MMN_ERR_INVALID_ARGUMENT: "invalid argument",
@@ -128,6 +130,9 @@ SIGNATURES = [
     ("mmn_cuda_sn_est_workspace_bytes", _SZ, [_I, _I]),
     ("mmn_cuda_sn_est", _I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _F,
                              _F, _F, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _SZ, _P]),
+    ("mmn_cuda_sn_est_fast", _I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                  _F, _F, _F, _I, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _SZ,
+                                  _P]),
     ("mmn_fp32_peak_probe", _I, [_I, _I, _P, _P]),
     ("mmn_wait_timeout_probe", _I, [ctypes.c_uint32, _I, _P, _P]),
     ("mmn_batch_create", _I, [_PROB, _I32, _I32, _P, _P, _I32, ctypes.POINTER(_P),

@@ -17,10 +17,9 @@ namespace mmn {
 namespace {
 constexpr int kInterpThreads = 256;
 constexpr int kInterpChunk = 256;  // antennas staged per shared-memory chunk
-const double kRefPi = 3.1415926535897932384626433832795028841971693993751058209749445923078164062862089986280348253421170679;
 
-struct RefContrib {
-    float sum_r, sum_i;
+struct Contrib {
+    float re, im;
     bool valid;
 };
 
@@ -36,37 +35,37 @@ __device__ __forceinline__ void load_meas(const InterpParams &p, unsigned idx, f
     }
 }
 
-// imaging_gpu.cu:70-105 -- the per-antenna contribution, same expressions.
-__device__ __forceinline__ RefContrib image_contrib(const InterpParams &p, unsigned i,
-                                                    float x_loc, float y_loc, float z_loc,
-                                                    float x_antenna_loc, float y_antenna_loc,
-                                                    float z_antenna_loc, float rx_offset_x,
-                                                    float rx_offset_y, float rx_offset_z) {
-    RefContrib r;
+// One (voxel, virtual antenna) term of imaging_gpu.cu:70-105 with the same floating-point
+// operations in the same order (FP32 legs and path, FP64 phase and cos/sin, FP32 complex
+// product), so the sums reproduce the reference kernel's bits.
+__device__ __forceinline__ Contrib pair_contrib(const InterpParams &p, unsigned i, float vx,
+                                                float vy, float vz, float tx, float ty,
+                                                float tz, float ox, float oy, float oz) {
+    Contrib r;
     r.valid = false;
-    float antenna_x_diff = x_loc - x_antenna_loc;
-    float antenna_y_diff = y_loc - y_antenna_loc;
-    float antenna_z_diff = z_loc - z_antenna_loc;
-    float forward_dist = sqrtf(antenna_x_diff * antenna_x_diff +
-                               antenna_y_diff * antenna_y_diff +
-                               antenna_z_diff * antenna_z_diff);
-    float back_dist = sqrtf((antenna_x_diff - rx_offset_x) * (antenna_x_diff - rx_offset_x) +
-                            (antenna_y_diff - rx_offset_y) * (antenna_y_diff - rx_offset_y) +
-                            (antenna_z_diff - rx_offset_z) * (antenna_z_diff - rx_offset_z));
-    float distance = forward_dist + back_dist;
+    float dx = vx - tx;
+    float dy = vy - ty;
+    float dz = vz - tz;
+    float leg_out = sqrtf(dx * dx +
+                          dy * dy +
+                          dz * dz);
+    float leg_back = sqrtf((dx - ox) * (dx - ox) +
+                           (dy - oy) * (dy - oy) +
+                           (dz - oz) * (dz - oz));
+    float path = leg_out + leg_back;
     if (p.is_ti != 0) {
-        distance += 0.15;
+        path += 0.15;
     }
-    if (distance < 0 || distance > p.fft_spacing * p.nbins) {
+    if (path < 0 || path > p.fft_spacing * p.nbins) {
         return r;
     }
-    int dist_bin = floorf(distance / p.fft_spacing / 2);
-    float real_meas, imag_meas;
-    load_meas(p, i * p.nbins + dist_bin, real_meas, imag_meas);
-    float real_phase = cos(-2 * kRefPi * distance / p.wavelength);
-    float imag_phase = sin(-2 * kRefPi * distance / p.wavelength);
-    r.sum_r = (real_meas * real_phase - imag_meas * imag_phase);
-    r.sum_i = (real_meas * imag_phase + imag_meas * real_phase);
+    int bin = floorf(path / p.fft_spacing / 2);
+    float m_re, m_im;
+    load_meas(p, i * p.nbins + bin, m_re, m_im);
+    float ph_re = cos(-2 * kPi * path / p.wavelength);
+    float ph_im = sin(-2 * kPi * path / p.wavelength);
+    r.re = (m_re * ph_re - m_im * ph_im);
+    r.im = (m_re * ph_im + m_im * ph_re);
     r.valid = true;
     return r;
 }
@@ -96,11 +95,11 @@ __global__ void __launch_bounds__(kInterpThreads) interp_image_kernel(const Inte
     const int x = (int)(v / nyz);
     const int y = (int)((v - (int64_t)x * nyz) / p.nz);
     const int z = (int)(v - (int64_t)x * nyz - (int64_t)y * p.nz);
-    const float x_loc = p.x_locs[x];
-    const float y_loc = p.y_locs[y];
-    const float z_loc = p.z_locs[z];
-    float sum_r = 0;
-    float sum_i = 0;
+    const float vx = p.x_locs[x];
+    const float vy = p.y_locs[y];
+    const float vz = p.z_locs[z];
+    float acc_re = 0;
+    float acc_im = 0;
     float w[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int a0 = 0; a0 < p.num_ant; a0 += kInterpChunk) {
         const int n = min(kInterpChunk, p.num_ant - a0);
@@ -110,30 +109,30 @@ __global__ void __launch_bounds__(kInterpThreads) interp_image_kernel(const Inte
         if (!active) continue;
         for (int j = 0; j < n; ++j) {
             const float *g = sh + 6 * j;
-            const RefContrib c = image_contrib(p, (unsigned)(a0 + j), x_loc, y_loc, z_loc, g[0],
-                                               g[1], g[2], g[3], g[4], g[5]);
+            const Contrib c = pair_contrib(p, (unsigned)(a0 + j), vx, vy, vz, g[0], g[1], g[2],
+                                           g[3], g[4], g[5]);
             if (!c.valid) continue;
-            sum_r += c.sum_r;
-            sum_i += c.sum_i;
+            acc_re += c.re;
+            acc_im += c.im;
             if (p.vote) {
-                const float vec_x = (g[0] + g[3] / 2) - x_loc;
-                const float vec_y = (g[1] + g[4] / 2) - y_loc;
-                const float vec_z = (g[2] + g[5] / 2) - z_loc;
-                w[0] = fmaf(c.sum_r, vec_x, w[0]);
-                w[1] = fmaf(c.sum_i, vec_x, w[1]);
-                w[2] = fmaf(c.sum_r, vec_y, w[2]);
-                w[3] = fmaf(c.sum_i, vec_y, w[3]);
-                w[4] = fmaf(c.sum_r, vec_z, w[4]);
-                w[5] = fmaf(c.sum_i, vec_z, w[5]);
+                const float ex = (g[0] + g[3] / 2) - vx;
+                const float ey = (g[1] + g[4] / 2) - vy;
+                const float ez = (g[2] + g[5] / 2) - vz;
+                w[0] = fmaf(c.re, ex, w[0]);
+                w[1] = fmaf(c.im, ex, w[1]);
+                w[2] = fmaf(c.re, ey, w[2]);
+                w[3] = fmaf(c.im, ey, w[3]);
+                w[4] = fmaf(c.re, ez, w[4]);
+                w[5] = fmaf(c.im, ez, w[5]);
             }
         }
     }
     if (!active) return;
     if (p.out_r) {
-        p.out_r[v] = sum_r;
-        p.out_i[v] = sum_i;
+        p.out_r[v] = acc_re;
+        p.out_i[v] = acc_im;
     }
-    if (p.image) p.image[v] = make_float2(sum_r, sum_i);
+    if (p.image) p.image[v] = make_float2(acc_re, acc_im);
     if (p.vote) {
         p.vote[v] = make_float2(w[0], w[1]);
         p.vote[p.nvox + v] = make_float2(w[2], w[3]);
@@ -141,7 +140,8 @@ __global__ void __launch_bounds__(kInterpThreads) interp_image_kernel(const Inte
     }
 }
 
-// Normal pass (cuda_sn_est, surface_normal_est.cu:63-149) over a valid-voxel list.
+// Normal pass (cuda_sn_est, surface_normal_est.cu:63-149) over a valid-voxel list; the
+// weight and the virtual-antenna direction use the reference's operations in order.
 __global__ void __launch_bounds__(kInterpThreads) interp_normals_kernel(const InterpParams p) {
     __shared__ float sh[6 * kInterpChunk];
     const int64_t rel = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -154,15 +154,15 @@ __global__ void __launch_bounds__(kInterpThreads) interp_normals_kernel(const In
         y = p.vidx_y[ind];
         z = p.vidx_z[ind];
     }
-    const float x_loc = p.x_locs[x];
-    const float y_loc = p.y_locs[y];
-    const float z_loc = p.z_locs[z];
-    const float image_r = active ? p.img_r[x * p.ny * p.nz + y * p.nz + z] : 1.f;
-    const float image_i = active ? p.img_i[x * p.ny * p.nz + y * p.nz + z] : 0.f;
-    const float image_mag = sqrtf(image_r * image_r + image_i * image_i);
-    float sn_x = 0;
-    float sn_y = 0;
-    float sn_z = 0;
+    const float vx = p.x_locs[x];
+    const float vy = p.y_locs[y];
+    const float vz = p.z_locs[z];
+    const float i_re = active ? p.img_r[x * p.ny * p.nz + y * p.nz + z] : 1.f;
+    const float i_im = active ? p.img_i[x * p.ny * p.nz + y * p.nz + z] : 0.f;
+    const float mag = sqrtf(i_re * i_re + i_im * i_im);
+    float acc_x = 0;
+    float acc_y = 0;
+    float acc_z = 0;
     for (int a0 = 0; a0 < p.num_ant; a0 += kInterpChunk) {
         const int n = min(kInterpChunk, p.num_ant - a0);
         __syncthreads();
@@ -171,31 +171,270 @@ __global__ void __launch_bounds__(kInterpThreads) interp_normals_kernel(const In
         if (!active) continue;
         for (int j = 0; j < n; ++j) {
             const float *g = sh + 6 * j;
-            const float x_antenna_loc = g[0], y_antenna_loc = g[1], z_antenna_loc = g[2];
-            const float rx_offset_x = g[3], rx_offset_y = g[4], rx_offset_z = g[5];
-            const RefContrib c = image_contrib(p, (unsigned)(a0 + j), x_loc, y_loc, z_loc,
-                                               x_antenna_loc, y_antenna_loc, z_antenna_loc,
-                                               rx_offset_x, rx_offset_y, rx_offset_z);
+            const float tx = g[0], ty = g[1], tz = g[2];
+            const float ox = g[3], oy = g[4], oz = g[5];
+            const Contrib c = pair_contrib(p, (unsigned)(a0 + j), vx, vy, vz, tx, ty, tz, ox,
+                                           oy, oz);
             if (!c.valid) continue;
-            float sum_r = c.sum_r;
-            float sum_i = c.sum_i;
-            float virtual_antenna_x = x_antenna_loc + rx_offset_x / 2;
-            float virtual_antenna_y = y_antenna_loc + rx_offset_y / 2;
-            float virtual_antenna_z = z_antenna_loc + rx_offset_z / 2;
-            float vec_x = virtual_antenna_x - x_loc;
-            float vec_y = virtual_antenna_y - y_loc;
-            float vec_z = virtual_antenna_z - z_loc;
-            float weight = (sum_r * image_r) + (sum_i * image_i);
-            weight /= image_mag;
-            sn_x += (vec_x * weight);
-            sn_y += (vec_y * weight);
-            sn_z += (vec_z * weight);
+            float c_re = c.re;
+            float c_im = c.im;
+            float ux = tx + ox / 2;
+            float uy = ty + oy / 2;
+            float uz = tz + oz / 2;
+            float ex = ux - vx;
+            float ey = uy - vy;
+            float ez = uz - vz;
+            float wgt = (c_re * i_re) + (c_im * i_im);
+            wgt /= mag;
+            acc_x += (ex * wgt);
+            acc_y += (ey * wgt);
+            acc_z += (ez * wgt);
         }
     }
     if (!active) return;
-    p.n_x[ind] = sn_x;
-    p.n_y[ind] = sn_y;
-    p.n_z[ind] = sn_z;
+    p.n_x[ind] = acc_x;
+    p.n_y[ind] = acc_y;
+    p.n_z[ind] = acc_z;
+}
+
+// ---------------------------------------------------------------------------------
+// Fast form.  The path length and the range bin are the reference's (same FP32
+// operations, so the same bin is gathered); only the phasor exp(-j 2 pi path/lambda) is
+// formed differently: instead of an FP64 cos and sin of the ~1e3-radian phase, the turn
+// count path/lambda is formed as a double-float product (1/lambda = hi + lo, both FP32;
+// the rounding error of path*hi recovered exactly by an FMA), its integer part removed
+// exactly, and the hardware sine/cosine (__sincosf, absolute error about 2^-21.4 on
+// [-pi, pi]) evaluated on the wrapped angle.  Phase error ~2e-7 turns + 4e-7 absolute in
+// each phasor component: about 5e-7 relative per term against the reference's phasor.
+// ---------------------------------------------------------------------------------
+namespace {
+constexpr int kFastT = 2;                  // voxels per thread
+constexpr float kRoundMagic = 12582912.f;  // 1.5 * 2^23: (x + M) - M rounds |x| < 2^22
+
+// Range antenna record of the fast kernels: TX, RX offset and the vote anchor TX + o/2
+// (formed in FP32 as surface_normal_est.cu:128-130 does).
+struct __align__(16) FastAnt {
+    float4 t, o, u;
+};
+
+__device__ __forceinline__ void stage_fast_chunk(const InterpParams &p, int a0, int n,
+                                                 FastAnt *sh) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int i = a0 + j;
+        const int rx = i % p.num_rx;
+        const float tx = p.ant[3 * i + 0], ty = p.ant[3 * i + 1], tz = p.ant[3 * i + 2];
+        const float ox = p.rxo[3 * rx + 0], oy = p.rxo[3 * rx + 1], oz = p.rxo[3 * rx + 2];
+        FastAnt a;
+        a.t = make_float4(tx, ty, tz, 0.f);
+        a.o = make_float4(ox, oy, oz, 0.f);
+        a.u = make_float4(tx + ox / 2, ty + oy / 2, tz + oz / 2, 0.f);
+        sh[j] = a;
+    }
+}
+
+// floor(RN(path / fsp) / 2), the reference's range bin (imaging_gpu.cu:100), for
+// 0 <= path <= fsp * nbins.  h = path * (1/(2 fsp)) is within 2e-7 h of the rounded
+// quotient's half, so floor(h) is that bin unless h lies within 1.2e-6 h of an integer;
+// then the reference's own division decides.  The floor comes from the rounding constant
+// (no conversion instruction): bits(h + M) - bits(M) = rint(h) for 0 <= h < 2^22.
+__device__ __forceinline__ int fast_bin(float path, float fsp, float half_inv) {
+    const float h = path * half_inv;
+    const float hm = h + kRoundMagic;
+    const float r = hm - kRoundMagic;
+    const int above = r > h ? 1 : 0;
+    const float fr = h - (r - (float)above);
+    const float tol = fmaxf(h, 1.f) * 1.2e-6f;
+    if (fr < tol || fr > 1.f - tol) return (int)floorf(path / fsp / 2);
+    return __float_as_int(hm) - __float_as_int(kRoundMagic) - above;
+}
+
+// (cos, sin) of -2 pi path / lambda with 1/lambda = hi + lo.
+__device__ __forceinline__ void fast_phasor(float path, float hi, float lo, float &c,
+                                            float &s) {
+    const float q = path * hi;
+    const float e = fmaf(path, hi, -q);        // exact: path*hi = q + e
+    const float n = (q + kRoundMagic) - kRoundMagic;
+    const float f = (q - n) + fmaf(path, lo, e);  // path/lambda - n; |f| <= 0.5 + ulp(q)
+    __sincosf(-6.28318530717958647692f * f, &s, &c);
+}
+
+template <bool MONO>
+__device__ __forceinline__ float2 fast_contrib(const InterpParams &p, size_t row, float vx,
+                                               float vy, float vz, const FastAnt &a,
+                                               float range_max) {
+    const float dx = vx - a.t.x;
+    const float dy = vy - a.t.y;
+    const float dz = vz - a.t.z;
+    const float leg_out = sqrtf(dx * dx +
+                                dy * dy +
+                                dz * dz);
+    float path;
+    if (MONO) {
+        path = leg_out + leg_out;  // the return leg with a zero offset is the same value
+    } else {
+        const float leg_back = sqrtf((dx - a.o.x) * (dx - a.o.x) +
+                                     (dy - a.o.y) * (dy - a.o.y) +
+                                     (dz - a.o.z) * (dz - a.o.z));
+        path = leg_out + leg_back;
+    }
+    if (p.is_ti != 0) {
+        path += 0.15;
+    }
+    const bool valid = !(path < 0 || path > range_max);
+    const int bin = valid ? fast_bin(path, p.fft_spacing, p.half_inv_fsp) : 0;
+    float m_re, m_im;
+    if (p.meas) {
+        const float2 m = __ldg(p.meas + row + bin);
+        m_re = m.x;
+        m_im = m.y;
+    } else {
+        m_re = __ldg(p.meas_r + row + bin);
+        m_im = __ldg(p.meas_i + row + bin);
+    }
+    float c, s;
+    fast_phasor(path, p.inv_lambda_hi, p.inv_lambda_lo, c, s);
+    const float re = fmaf(m_re, c, -m_im * s);
+    const float im = fmaf(m_re, s, m_im * c);
+    return valid ? make_float2(re, im) : make_float2(0.f, 0.f);
+}
+
+// Does any staged antenna of this chunk have a non-zero RX offset?  (Uniform per CTA.)
+__device__ __forceinline__ bool chunk_has_offsets(const FastAnt *sh, int n) {
+    bool any = false;
+    for (int j = threadIdx.x; j < n; j += blockDim.x)
+        any |= (sh[j].o.x != 0.f) | (sh[j].o.y != 0.f) | (sh[j].o.z != 0.f);
+    return __syncthreads_or(any) != 0;
+}
+
+template <bool MONO, bool VOTE>
+__device__ __forceinline__ void fast_image_chunk(const InterpParams &p, const FastAnt *sh,
+                                                 int a0, int n, float range_max,
+                                                 const float (&vx)[kFastT],
+                                                 const float (&vy)[kFastT],
+                                                 const float (&vz)[kFastT],
+                                                 float (&acc)[kFastT][8]) {
+#pragma unroll 2
+    for (int j = 0; j < n; ++j) {
+        const FastAnt a = sh[j];
+        const size_t row = (size_t)(a0 + j) * (size_t)p.nbins;
+#pragma unroll
+        for (int k = 0; k < kFastT; ++k) {
+            const float2 c = fast_contrib<MONO>(p, row, vx[k], vy[k], vz[k], a, range_max);
+            acc[k][0] += c.x;
+            acc[k][1] += c.y;
+            if (VOTE) {
+                const float ex = a.u.x - vx[k], ey = a.u.y - vy[k], ez = a.u.z - vz[k];
+                acc[k][2] = fmaf(c.x, ex, acc[k][2]);
+                acc[k][3] = fmaf(c.y, ex, acc[k][3]);
+                acc[k][4] = fmaf(c.x, ey, acc[k][4]);
+                acc[k][5] = fmaf(c.y, ey, acc[k][5]);
+                acc[k][6] = fmaf(c.x, ez, acc[k][6]);
+                acc[k][7] = fmaf(c.y, ez, acc[k][7]);
+            }
+        }
+    }
+}
+}  // namespace
+
+// Image pass in fast form, kFastT voxels per thread (strided by the block size so loads
+// and stores coalesce), optionally fusing the vote vector.
+__global__ void __launch_bounds__(kInterpThreads) interp_image_fast_kernel(const InterpParams p) {
+    __shared__ FastAnt sh[kInterpChunk];
+    const int64_t nyz = (int64_t)p.ny * p.nz;
+    const float range_max = p.fft_spacing * p.nbins;
+    int64_t vox[kFastT];
+    bool active[kFastT];
+    float vx[kFastT], vy[kFastT], vz[kFastT];
+    float acc[kFastT][8];
+#pragma unroll
+    for (int k = 0; k < kFastT; ++k) {
+        const int64_t rel = ((int64_t)blockIdx.x * kFastT + k) * blockDim.x + threadIdx.x;
+        active[k] = rel < p.count && rel + p.start < p.nvox;
+        const int64_t v = active[k] ? rel + p.start : 0;
+        vox[k] = v;
+        const int x = (int)(v / nyz);
+        const int y = (int)((v - (int64_t)x * nyz) / p.nz);
+        const int z = (int)(v - (int64_t)x * nyz - (int64_t)y * p.nz);
+        vx[k] = p.x_locs[x];
+        vy[k] = p.y_locs[y];
+        vz[k] = p.z_locs[z];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[k][q] = 0.f;
+    }
+    for (int a0 = 0; a0 < p.num_ant; a0 += kInterpChunk) {
+        const int n = min(kInterpChunk, p.num_ant - a0);
+        __syncthreads();
+        stage_fast_chunk(p, a0, n, sh);
+        __syncthreads();
+        const bool offsets = chunk_has_offsets(sh, n);
+        if (p.vote) {
+            if (offsets) fast_image_chunk<false, true>(p, sh, a0, n, range_max, vx, vy, vz, acc);
+            else fast_image_chunk<true, true>(p, sh, a0, n, range_max, vx, vy, vz, acc);
+        } else {
+            if (offsets) fast_image_chunk<false, false>(p, sh, a0, n, range_max, vx, vy, vz, acc);
+            else fast_image_chunk<true, false>(p, sh, a0, n, range_max, vx, vy, vz, acc);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kFastT; ++k) {
+        if (!active[k]) continue;
+        const int64_t v = vox[k];
+        if (p.out_r) {
+            p.out_r[v] = acc[k][0];
+            p.out_i[v] = acc[k][1];
+        }
+        if (p.image) p.image[v] = make_float2(acc[k][0], acc[k][1]);
+        if (p.vote) {
+            p.vote[v] = make_float2(acc[k][2], acc[k][3]);
+            p.vote[p.nvox + v] = make_float2(acc[k][4], acc[k][5]);
+            p.vote[2 * p.nvox + v] = make_float2(acc[k][6], acc[k][7]);
+        }
+    }
+}
+
+// Normal pass in fast form over a valid-voxel list (one voxel per thread).
+__global__ void __launch_bounds__(kInterpThreads) interp_normals_fast_kernel(const InterpParams p) {
+    __shared__ FastAnt sh[kInterpChunk];
+    const int64_t rel = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t ind64 = rel + p.start;
+    const bool active = rel < p.count && ind64 < p.num_valid && ind64 >= 0;
+    const int ind = active ? (int)ind64 : 0;
+    int x = 0, y = 0, z = 0;
+    if (active) {
+        x = p.vidx_x[ind];
+        y = p.vidx_y[ind];
+        z = p.vidx_z[ind];
+    }
+    const float vx = p.x_locs[x], vy = p.y_locs[y], vz = p.z_locs[z];
+    const int64_t v = ((int64_t)x * p.ny + y) * p.nz + z;
+    const float i_re = active ? p.img_r[v] : 1.f;
+    const float i_im = active ? p.img_i[v] : 0.f;
+    const float inv_mag = 1.f / sqrtf(i_re * i_re + i_im * i_im);
+    const float range_max = p.fft_spacing * p.nbins;
+    float acc_x = 0.f, acc_y = 0.f, acc_z = 0.f;
+    for (int a0 = 0; a0 < p.num_ant; a0 += kInterpChunk) {
+        const int n = min(kInterpChunk, p.num_ant - a0);
+        __syncthreads();
+        stage_fast_chunk(p, a0, n, sh);
+        __syncthreads();
+        const bool offsets = chunk_has_offsets(sh, n);
+        if (!active) continue;
+#pragma unroll 2
+        for (int j = 0; j < n; ++j) {
+            const FastAnt a = sh[j];
+            const size_t row = (size_t)(a0 + j) * (size_t)p.nbins;
+            const float2 c = offsets ? fast_contrib<false>(p, row, vx, vy, vz, a, range_max)
+                                     : fast_contrib<true>(p, row, vx, vy, vz, a, range_max);
+            const float wgt = fmaf(c.x, i_re, c.y * i_im) * inv_mag;
+            acc_x = fmaf(a.u.x - vx, wgt, acc_x);
+            acc_y = fmaf(a.u.y - vy, wgt, acc_y);
+            acc_z = fmaf(a.u.z - vz, wgt, acc_z);
+        }
+    }
+    if (!active) return;
+    p.n_x[ind] = acc_x;
+    p.n_y[ind] = acc_y;
+    p.n_z[ind] = acc_z;
 }
 
 cudaError_t launch_interp_image(const InterpParams &p, cudaStream_t stream) {
@@ -209,6 +448,21 @@ cudaError_t launch_interp_normals(const InterpParams &p, cudaStream_t stream) {
     if (p.count <= 0) return cudaSuccess;
     const int64_t blocks = (p.count + kInterpThreads - 1) / kInterpThreads;
     interp_normals_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_interp_image_fast(const InterpParams &p, cudaStream_t stream) {
+    if (p.count <= 0) return cudaSuccess;
+    const int64_t per = (int64_t)kInterpThreads * kFastT;
+    const int64_t blocks = (p.count + per - 1) / per;
+    interp_image_fast_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_interp_normals_fast(const InterpParams &p, cudaStream_t stream) {
+    if (p.count <= 0) return cudaSuccess;
+    const int64_t blocks = (p.count + kInterpThreads - 1) / kInterpThreads;
+    interp_normals_fast_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
     return cudaGetLastError();
 }
 

@@ -160,10 +160,17 @@ struct InterpParams {
     float *n_x, *n_y, *n_z;
     int32_t num_valid;
     int32_t pad1;
+    // fast form only: 1/lambda split into two floats (hi + lo) and 1/(2 fft_spacing)
+    float inv_lambda_hi, inv_lambda_lo, half_inv_fsp;
+    int32_t mono;            // 1 when every RX offset is zero (fast form)
 };
 
 cudaError_t launch_interp_image(const InterpParams &p, cudaStream_t stream);
 cudaError_t launch_interp_normals(const InterpParams &p, cudaStream_t stream);
+// fast form of both passes: same path length and range bin as the reference, the
+// phasor from a wrapped FP32 turn count and the hardware sine/cosine
+cudaError_t launch_interp_image_fast(const InterpParams &p, cudaStream_t stream);
+cudaError_t launch_interp_normals_fast(const InterpParams &p, cudaStream_t stream);
 
 // --------------------------------------------------------------------- epilogue
 cudaError_t launch_max_abs(int64_t nvox, const float2 *image, unsigned int *max_bits,

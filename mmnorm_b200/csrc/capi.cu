@@ -26,6 +26,7 @@ namespace {
 constexpr size_t kAlign = 256;
 constexpr int kMaxStageBytes = 48 * 1024;
 constexpr int kMaxFp = 24576;  // one antenna row per stage still fits in shared memory
+constexpr int kMaxFastBins = 1 << 22;  // fast interpolated form: rounding-constant bins
 
 inline size_t align_up(size_t x, size_t a = kAlign) { return (x + a - 1) / a * a; }
 
@@ -44,14 +45,17 @@ int variant_index_for(int mode) { return g_variant[mode == MMN_MODE_PLAIN ? 1 : 
 
 int check_problem(const mmn_problem *p, int mode) {
     if (!p) return MMN_ERR_NULL_POINTER;
-    if (mode != MMN_MODE_MIXED && mode != MMN_MODE_PLAIN && mode != MMN_MODE_INTERP)
+    if (mode != MMN_MODE_MIXED && mode != MMN_MODE_PLAIN && mode != MMN_MODE_INTERP &&
+        mode != MMN_MODE_INTERP_FAST)
         return MMN_ERR_INVALID_ARGUMENT;
     if (p->num_x < 1 || p->num_y < 1 || p->num_z < 1) return MMN_ERR_INVALID_ARGUMENT;
     if (p->num_antennas < 0 || p->num_rx < 1 || p->num_samples < 1)
         return MMN_ERR_INVALID_ARGUMENT;
     if (!(p->wavelength > 0.0) || !std::isfinite(p->wavelength) || !std::isfinite(p->slope))
         return MMN_ERR_INVALID_ARGUMENT;
-    if (mode == MMN_MODE_INTERP && !(p->fft_spacing > 0.0)) return MMN_ERR_INVALID_ARGUMENT;
+    if ((mode == MMN_MODE_INTERP || mode == MMN_MODE_INTERP_FAST) && !(p->fft_spacing > 0.0))
+        return MMN_ERR_INVALID_ARGUMENT;
+    if (mode == MMN_MODE_INTERP_FAST && p->num_samples > kMaxFastBins) return MMN_ERR_TOO_LARGE;
     if (!p->x_locs || !p->y_locs || !p->z_locs) return MMN_ERR_NULL_POINTER;
     if (p->num_antennas > 0 && (!p->antenna_locs || !p->rx_offsets || !p->meas))
         return MMN_ERR_NULL_POINTER;
@@ -198,6 +202,18 @@ int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
 
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+bool is_interp(int mode) { return mode == MMN_MODE_INTERP || mode == MMN_MODE_INTERP_FAST; }
+
+// Constants of the interpolated mode's fast form: 1/lambda as the sum of two floats (the
+// reference forms its phase from the FP32 wavelength promoted to FP64) and 1/(2 fft_spacing)
+// from the correctly rounded FP32 reciprocal.
+void set_fast_fields(InterpParams &ip) {
+    const double inv = 1.0 / (double)ip.wavelength;
+    ip.inv_lambda_hi = (float)inv;
+    ip.inv_lambda_lo = (float)(inv - (double)ip.inv_lambda_hi);
+    ip.half_inv_fsp = 0.5f * (1.0f / ip.fft_spacing);
+}
+
 }  // namespace
 
 extern "C" {
@@ -265,7 +281,7 @@ const char *mmn_variant_name(int32_t mode, int32_t idx) {
 size_t mmn_workspace_bytes(const mmn_problem *p, int32_t mode, int32_t want_vote) {
     (void)want_vote;
     if (check_problem(p, mode) != MMN_OK) return 0;
-    if (mode == MMN_MODE_INTERP) return kStatusBytes;
+    if (is_interp(mode)) return kStatusBytes;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     FwdPlan pl;
     if (plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode, aligned16(p->meas),
@@ -278,7 +294,7 @@ int mmn_plan_info(const mmn_problem *p, int32_t mode, int32_t *tiles, int32_t *s
                   int32_t *ant_per_stage, int32_t *threads, int32_t *voxels_per_thread) {
     int rc = check_problem(p, mode);
     if (rc != MMN_OK) return rc;
-    if (mode == MMN_MODE_INTERP) return MMN_ERR_INVALID_ARGUMENT;
+    if (is_interp(mode)) return MMN_ERR_INVALID_ARGUMENT;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     FwdPlan pl;
     rc = plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode, aligned16(p->meas),
@@ -307,7 +323,7 @@ int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vot
         return MMN_OK;
     }
     unsigned char *ws = static_cast<unsigned char *>(workspace);
-    if (mode == MMN_MODE_INTERP) {
+    if (is_interp(mode)) {
         if (workspace_bytes < kStatusBytes) return MMN_ERR_WORKSPACE;
         if (reinterpret_cast<uintptr_t>(p->meas) & 7u) return MMN_ERR_INVALID_ARGUMENT;
         if (cudaMemsetAsync(ws, 0, 16, stream) != cudaSuccess) return MMN_ERR_CUDA;
@@ -334,6 +350,10 @@ int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vot
         ip.image = reinterpret_cast<float2 *>(image);
         ip.vote = reinterpret_cast<float2 *>(vote);
         if (p->pos_offsets) return MMN_ERR_UNSUPPORTED;
+        if (mode == MMN_MODE_INTERP_FAST) {
+            set_fast_fields(ip);
+            return launch_interp_image_fast(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+        }
         return launch_interp_image(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
     }
     FwdPlan pl;
@@ -479,6 +499,11 @@ int mmn_cuda_image(float *p_xyz_r, float *p_xyz_i, const float *x_locs, const fl
         ip.nvox = nvox;
         ip.out_r = p_xyz_r;
         ip.out_i = p_xyz_i;
+        if (use_interpolated_processing == 2) {
+            if (samples_per_meas > kMaxFastBins) return MMN_ERR_TOO_LARGE;
+            set_fast_fields(ip);
+            return launch_interp_image_fast(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+        }
         return launch_interp_image(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
     }
     mmn_problem p;
@@ -511,15 +536,18 @@ size_t mmn_cuda_sn_est_workspace_bytes(int num_antennas, int samples_per_meas) {
     return kStatusBytes;
 }
 
-int mmn_cuda_sn_est(float *normals_x, float *normals_y, float *normals_z, const int *valid_idx_x,
-                    const int *valid_idx_y, const int *valid_idx_z, const float *p_xyz_r,
-                    const float *p_xyz_i, const float *x_locs, const float *y_locs,
-                    const float *z_locs, const float *antenna_locs, const float *meas_r,
-                    const float *meas_i, const float *rx_offsets, float slope, float wavelength,
-                    float fft_spacing, int num_x, int num_y, int num_z, int num_antennas,
-                    int num_rx_antennas, int num_valid_idx, int samples_per_meas, int start_ind,
-                    int is_ti_radar, int count, void *workspace, size_t workspace_bytes,
-                    cudaStream_t stream) {
+}  // extern "C"
+
+namespace {
+int cuda_sn_est_impl(bool fast, float *normals_x, float *normals_y, float *normals_z,
+                     const int *valid_idx_x, const int *valid_idx_y, const int *valid_idx_z,
+                     const float *p_xyz_r, const float *p_xyz_i, const float *x_locs,
+                     const float *y_locs, const float *z_locs, const float *antenna_locs,
+                     const float *meas_r, const float *meas_i, const float *rx_offsets,
+                     float slope, float wavelength, float fft_spacing, int num_x, int num_y,
+                     int num_z, int num_antennas, int num_rx_antennas, int num_valid_idx,
+                     int samples_per_meas, int start_ind, int is_ti_radar, int count,
+                     void *workspace, size_t workspace_bytes, cudaStream_t stream) {
     (void)slope;
     (void)workspace;
     (void)workspace_bytes;
@@ -564,7 +592,49 @@ int mmn_cuda_sn_est(float *normals_x, float *normals_y, float *normals_z, const 
     ip.n_y = normals_y;
     ip.n_z = normals_z;
     ip.num_valid = num_valid_idx;
+    if (fast) {
+        if (samples_per_meas > kMaxFastBins) return MMN_ERR_TOO_LARGE;
+        set_fast_fields(ip);
+        return launch_interp_normals_fast(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+    }
     return launch_interp_normals(ip, stream) == cudaSuccess ? MMN_OK : MMN_ERR_CUDA;
+}
+}  // namespace
+
+extern "C" {
+
+int mmn_cuda_sn_est(float *normals_x, float *normals_y, float *normals_z, const int *valid_idx_x,
+                    const int *valid_idx_y, const int *valid_idx_z, const float *p_xyz_r,
+                    const float *p_xyz_i, const float *x_locs, const float *y_locs,
+                    const float *z_locs, const float *antenna_locs, const float *meas_r,
+                    const float *meas_i, const float *rx_offsets, float slope, float wavelength,
+                    float fft_spacing, int num_x, int num_y, int num_z, int num_antennas,
+                    int num_rx_antennas, int num_valid_idx, int samples_per_meas, int start_ind,
+                    int is_ti_radar, int count, void *workspace, size_t workspace_bytes,
+                    cudaStream_t stream) {
+    return cuda_sn_est_impl(false, normals_x, normals_y, normals_z, valid_idx_x, valid_idx_y,
+                            valid_idx_z, p_xyz_r, p_xyz_i, x_locs, y_locs, z_locs, antenna_locs,
+                            meas_r, meas_i, rx_offsets, slope, wavelength, fft_spacing, num_x,
+                            num_y, num_z, num_antennas, num_rx_antennas, num_valid_idx,
+                            samples_per_meas, start_ind, is_ti_radar, count, workspace,
+                            workspace_bytes, stream);
+}
+
+int mmn_cuda_sn_est_fast(float *normals_x, float *normals_y, float *normals_z,
+                         const int *valid_idx_x, const int *valid_idx_y, const int *valid_idx_z,
+                         const float *p_xyz_r, const float *p_xyz_i, const float *x_locs,
+                         const float *y_locs, const float *z_locs, const float *antenna_locs,
+                         const float *meas_r, const float *meas_i, const float *rx_offsets,
+                         float slope, float wavelength, float fft_spacing, int num_x, int num_y,
+                         int num_z, int num_antennas, int num_rx_antennas, int num_valid_idx,
+                         int samples_per_meas, int start_ind, int is_ti_radar, int count,
+                         void *workspace, size_t workspace_bytes, cudaStream_t stream) {
+    return cuda_sn_est_impl(true, normals_x, normals_y, normals_z, valid_idx_x, valid_idx_y,
+                            valid_idx_z, p_xyz_r, p_xyz_i, x_locs, y_locs, z_locs, antenna_locs,
+                            meas_r, meas_i, rx_offsets, slope, wavelength, fft_spacing, num_x,
+                            num_y, num_z, num_antennas, num_rx_antennas, num_valid_idx,
+                            samples_per_meas, start_ind, is_ti_radar, count, workspace,
+                            workspace_bytes, stream);
 }
 
 int mmn_read_status(void *workspace, int32_t *status, cudaStream_t stream) {
@@ -1128,7 +1198,7 @@ extern "C" int mmn_backproject_noalloc(const mmn_problem *p, int32_t mode, float
     if (!image) return MMN_ERR_NULL_POINTER;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     FwdPlan pl;
-    const bool full = mode != MMN_MODE_INTERP && p->num_antennas > 0;
+    const bool full = !is_interp(mode) && p->num_antennas > 0;
     if (full) {
         rc = plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode,
                           aligned16(p->meas), false, &pl);

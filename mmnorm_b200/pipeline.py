@@ -7,8 +7,10 @@
     normals /= ||normals||                               # :396
 
 For the full matched filter this is ONE fused device pass (image and vote together),
-where the reference runs two kernels.  For interpolated mode it runs the reference's
-two-pass arithmetic (image, then the vote on the valid voxels).  The outputs are the
+where the reference runs two kernels, and the unit normals are formed on the device
+from the vote, which never leaves it.  For interpolated mode it runs the reference's
+two-pass arithmetic (image, then the vote on the valid voxels), or with
+``precision="fast"`` the fast form of both passes.  The outputs are the
 same objects the reference produces: complex64 image normalised as image_cuda does,
 float64 unit normals with NaN outside the mask, and the virtual phase centres.
 """
@@ -28,21 +30,24 @@ def surface_normals(x_locs, y_locs, z_locs, antenna_locs, measurement_data, rx_o
         sum_image, center_locs = py_image_gpu.image_cuda(
             x_locs, y_locs, z_locs, antenna_locs, measurement_data, rx_offsets, slope,
             wavelength, bandwidth, num_samples, use_4_rx=use_4_rx, is_ti_radar=is_ti_radar,
-            use_interpolated_processing=True)
+            use_interpolated_processing=True, precision=precision)
         normals = py_sn_est_gpu.normal_estimates_cuda(
             sum_image, x_locs, y_locs, z_locs, antenna_locs, measurement_data, rx_offsets,
             slope, wavelength, bandwidth, num_samples, use_4_rx=use_4_rx,
             is_ti_radar=is_ti_radar, initial_filter_percent=initial_filter_percent,
-            use_interpolated_processing=True)
+            use_interpolated_processing=True, precision=precision)
     else:
         image, norm_factor, locs_rep, vote = py_image_gpu.run_cuda_image(
             x_locs, y_locs, z_locs, antenna_locs, measurement_data, rx_offsets, slope,
             wavelength, bandwidth, num_samples, use_4_rx, is_ti_radar, False, precision,
-            want_vote=True)
+            want_vote=True, vote_on_device=True)
         sum_image = image
         sum_image /= norm_factor
         center_locs = py_image_gpu._centres(locs_rep, rx_offsets)
-        normals = py_sn_est_gpu.raw_normals_from_vote(sum_image, vote, initial_filter_percent)
+        # unit normals formed on the device from the vote that never left it
+        normals = py_sn_est_gpu.raw_normals_from_vote(sum_image, vote, initial_filter_percent,
+                                                      unit=True)
+        return sum_image, normals, center_locs
     with np.errstate(invalid="ignore", divide="ignore"):
         normals /= np.linalg.norm(normals, axis=-1)[..., np.newaxis].repeat(3, axis=-1)
     return sum_image, normals, center_locs

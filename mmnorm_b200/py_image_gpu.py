@@ -16,7 +16,10 @@ and the full matched filter runs the mixed-precision kernel (FP64 range and phas
 wrap, FP32 rotation recurrence) instead of one FP64 sin/cos pair per sample.
 ``precision='plain'`` selects the FP32 sincos-per-sample kernel instead, and
 ``precision='nufft'`` the same sums by 8-tap interpolation from per-antenna oversampled
-grids (~2e-6 from the mixed form, faster for F above ~100; F up to ~1500).
+grids (~2e-6 from the mixed form, faster for F above ~100; F up to ~1500).  In
+interpolated mode the default is the reference's arithmetic bit for bit, and
+``precision='fast'`` the fast form: the same range bins, the phasor from the wrapped
+FP32 turn count and the hardware sine/cosine (~5e-7 per term from the reference's).
 """
 from __future__ import annotations
 
@@ -61,11 +64,13 @@ def _rows(measurements, samples_per_meas, num_ant):
 
 def run_cuda_image(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offset, slope,
                    wavelength, bandwidth, num_samples, use_4_rx=False, is_ti_radar=False,
-                   use_interpolated_processing=False, precision="mixed", want_vote=False):
+                   use_interpolated_processing=False, precision="mixed", want_vote=False,
+                   vote_on_device=False):
     """py_image_gpu._run_cuda_image (py_image_gpu.py:237-305): one device pass.
 
     Returns (image complex64 [NX,NY,NZ] divided once by the TX count, norm_factor,
-    repeated antenna locations, vote complex64 [3,NX,NY,NZ] (raw, or None))."""
+    repeated antenna locations, vote complex64 [3,NX,NY,NZ] (raw, or None); a device
+    tensor with ``vote_on_device``)."""
     dev = _device()
     norm_factor = antenna_locs.shape[0]
     samples_per_meas = radar_data.shape[1]
@@ -76,7 +81,10 @@ def run_cuda_image(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offset, 
     fft_spacing = np.float32(3e8 / (2 * bandwidth) * num_samples / (radar_data.shape[1]))
     f32 = lambda a: torch.as_tensor(np.ascontiguousarray(np.asarray(a, dtype=np.float32)),
                                     device=dev)
-    mode = "interp" if use_interpolated_processing else precision
+    if use_interpolated_processing:
+        mode = "interp_fast" if precision == "fast" else "interp"
+    else:
+        mode = precision
     image, vote = ops.backproject(
         f32(x_locs), f32(y_locs), f32(z_locs), f32(np.asarray(antenna_locs).reshape(-1, 3)),
         f32(np.asarray(rx_offset_flat).reshape(-1, 3)), torch.as_tensor(rows, device=dev),
@@ -84,7 +92,9 @@ def run_cuda_image(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offset, 
         fft_spacing=float(fft_spacing), is_ti_radar=bool(is_ti_radar), want_vote=want_vote)
     p_xyz = image.cpu().numpy()
     p_xyz /= norm_factor
-    return p_xyz, norm_factor, antenna_locs, (vote.cpu().numpy() if vote is not None else None)
+    if vote is not None and not vote_on_device:
+        vote = vote.cpu().numpy()
+    return p_xyz, norm_factor, antenna_locs, vote
 
 
 def _centres(locs_rep, rx_offsets):
@@ -115,7 +125,7 @@ def image_cuda(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offsets, slo
             sl = slice(i * MAX_NUM_ANT // num_rx, (i + 1) * MAX_NUM_ANT // num_rx)
             image_subset, _, locs_rep, _ = run_cuda_image(
                 x_locs, y_locs, z_locs, antenna_locs[sl], radar_data[sl], rx_offsets, slope,
-                wavelength, bandwidth, num_samples, use_4_rx, is_ti_radar, True)
+                wavelength, bandwidth, num_samples, use_4_rx, is_ti_radar, True, precision)
             if return_phase_centers:
                 center_locs_subset = _centres(locs_rep, rx_offsets)
             if i == 0:

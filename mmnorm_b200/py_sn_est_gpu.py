@@ -35,16 +35,23 @@ def prep_inputs(radar_data, rx_offset, antenna_locs, use_4_rx):
     return rx_offset, radar_data, antenna_locs
 
 
+def _mask(sum_image, initial_filter_percent):
+    """|I| > initial_filter_percent * max|I| (py_sn_est_gpu.py:326)."""
+    mag = np.abs(sum_image)
+    return mag > (np.max(mag) * initial_filter_percent)
+
+
 def _mask_and_coords(sum_image, initial_filter_percent):
-    filter_idx = np.abs(sum_image) > (np.max(np.abs(sum_image)) * initial_filter_percent)
+    filter_idx = _mask(sum_image, initial_filter_percent)
     coords = np.argwhere(filter_idx)  # C order == the reference's meshgrid order
     return filter_idx, coords
 
 
 def sn_est_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offset, slope,
                 wavelength, bandwidth, num_samples, use_4_rx=False, is_ti_radar=False,
-                initial_filter_percent=0.05):
-    """py_sn_est_gpu._sn_est_cuda (py_sn_est_gpu.py:291-379) for one antenna group."""
+                initial_filter_percent=0.05, precision="exact"):
+    """py_sn_est_gpu._sn_est_cuda (py_sn_est_gpu.py:291-379) for one antenna group;
+    ``precision="fast"`` runs the fast form of the vote (mmn_cuda_sn_est_fast)."""
     dev = _device()
     samples_per_meas = radar_data.shape[1]
     rx_offset_flat, measurements, antenna_locs = prep_inputs(radar_data, rx_offset,
@@ -81,7 +88,9 @@ def sn_est_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_
     ws_bytes = max(256, _lib.load().mmn_cuda_sn_est_workspace_bytes(num_ant, samples_per_meas))
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     vp = ops._vp
-    rc = _lib.load().mmn_cuda_sn_est(
+    entry = _lib.load().mmn_cuda_sn_est_fast if precision == "fast" else \
+        _lib.load().mmn_cuda_sn_est
+    rc = entry(
         vp(keep["nx"]), vp(keep["ny"]), vp(keep["nz"]), vp(keep["vx"]), vp(keep["vy"]),
         vp(keep["vz"]), vp(keep["ir"]), vp(keep["ii"]), vp(keep["x"]), vp(keep["y"]),
         vp(keep["z"]), vp(keep["ant"]), vp(keep["mr"]), vp(keep["mi"]), vp(keep["rxo"]),
@@ -94,20 +103,27 @@ def sn_est_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_
     return all_normals
 
 
-def raw_normals_from_vote(sum_image, vote, initial_filter_percent=0.05):
-    """Reference-layout normals (float64, NaN outside the mask, not unit) from the fused
-    vote: n = Re(conj(I) W)/|I| with I the given image cast to float32 as the reference
-    passes it to the kernel (py_sn_est_gpu.py:236-237)."""
+def raw_normals_from_vote(sum_image, vote, initial_filter_percent=0.05, unit=False):
+    """Reference-layout normals (float64, NaN outside the mask) from the fused vote:
+    n = Re(conj(I) W)/|I| with I the given image cast to float32 as the reference passes it
+    to the kernel (py_sn_est_gpu.py:236-237); ``unit`` also divides by |n| (the caller's
+    step at image_processor.py:396).  ``vote`` is the complex64 [3, ...] vote, preferably
+    still on the device.  The normals are formed on the GPU and come back as one float32
+    [V, 3] array; the mask |I| > initial_filter_percent * max|I| is taken on the host in
+    the image's own dtype, exactly as py_sn_est_gpu.py:326 does."""
     sum_image = np.asarray(sum_image)
-    filter_idx, _ = _mask_and_coords(sum_image, initial_filter_percent)
-    ir = np.real(sum_image).astype(np.float32).astype(np.float64)
-    ii = np.imag(sum_image).astype(np.float32).astype(np.float64)
-    mag = np.sqrt(ir * ir + ii * ii)
-    sel = filter_idx
-    w = np.asarray(vote)[:, sel]                                       # [3, nvalid]
-    n = (ir[sel][None] * np.real(w) + ii[sel][None] * np.imag(w)) / mag[sel][None]
-    out = np.full(sum_image.shape + (3,), np.nan)
-    out[sel] = n.T
+    filter_idx = _mask(sum_image, initial_filter_percent)
+    dev = _device()
+    V = sum_image.size
+    img = torch.as_tensor(np.ascontiguousarray(sum_image.reshape(-1), dtype=np.complex64),
+                          device=dev)
+    w = vote if torch.is_tensor(vote) else torch.as_tensor(np.ascontiguousarray(vote), device=dev)
+    w = w.to(dev).reshape(3, V)
+    # filter 0: every voxel with |I| > 0 gets its normal; the host mask then decides
+    normals, _, raw = ops.surface_normals(img, w, 0.0, want_raw=True)
+    src = normals if unit else raw
+    out = src.cpu().numpy().astype(np.float64).reshape(sum_image.shape + (3,))
+    out[~filter_idx] = np.nan
     return out
 
 
@@ -116,11 +132,15 @@ def normal_estimates_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs, radar
                           is_ti_radar=False, initial_filter_percent=0.05,
                           use_interpolated_processing=True, precision="mixed"):
     """mmWave surface-normal estimates; same contract as the reference
-    (py_sn_est_gpu.py:382-424), plus the full matched filter."""
+    (py_sn_est_gpu.py:382-424), plus the full matched filter.  ``precision``: for the full
+    matched filter 'mixed' (default), 'plain' or 'nufft'; for interpolated mode 'fast'
+    selects the fast form (the reference's bins, hardware sine/cosine phasor, ~5e-7 from
+    the reference arithmetic), anything else the reference's arithmetic bit for bit."""
     if not use_interpolated_processing:
         _, _, _, vote = run_cuda_image(x_locs, y_locs, z_locs, antenna_locs, radar_data,
                                        rx_offset, slope, wavelength, bandwidth, num_samples,
-                                       use_4_rx, is_ti_radar, False, precision, want_vote=True)
+                                       use_4_rx, is_ti_radar, False, precision, want_vote=True,
+                                       vote_on_device=True)
         return raw_normals_from_vote(sum_image, vote, initial_filter_percent)
     num_rx = len(rx_offset)
     groups = math.ceil(antenna_locs.shape[0] * num_rx / MAX_NUM_ANT)
@@ -129,6 +149,6 @@ def normal_estimates_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs, radar
         sl = slice(i * MAX_NUM_ANT // num_rx, (i + 1) * MAX_NUM_ANT // num_rx)
         part = sn_est_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs[sl], radar_data[sl],
                            rx_offset, slope, wavelength, bandwidth, num_samples, use_4_rx,
-                           is_ti_radar, initial_filter_percent)
+                           is_ti_radar, initial_filter_percent, precision)
         normals = part if normals is None else normals + part
     return normals

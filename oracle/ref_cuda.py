@@ -87,3 +87,57 @@ def cuda_sn_est(n_x, n_y, n_z, vx, vy, vz, p_r, p_i, x, y, z, ant, mr, mi, rxo, 
             int(num_ant), int(num_rx), int(num_valid), int(samples), int(start_ind), int(is_ti)]
     types = [P] * 15 + [F] * 3 + [I] * 9
     _launch(fn, grid, block, args, types)
+
+
+class _DevPtr:
+    """A raw device address with the data_ptr() accessor the launchers read."""
+
+    def __init__(self, ptr):
+        self.ptr = int(ptr)
+
+    def data_ptr(self):
+        return self.ptr
+
+
+def cuda_image_in_out(x, y, z, ant, meas_r, meas_i, rxo, slope, wavelength, fft_spacing,
+                      num_ant, num_rx, samples, is_ti, interp):
+    """cuda_image with the reference's per-call transfers (py_image_gpu.py:189-199): each
+    input through pycuda's drv.In -- a device allocation and a synchronous copy from the
+    caller's (pageable) numpy array -- and the two outputs through drv.Out (allocation,
+    launch, synchronous copy back), all freed before return.  Host numpy in, (p_r, p_i)
+    float32 numpy out.  The per-call SourceModule build (py_image_gpu.py:56-179) is not
+    included: pycuda serves it from its on-disk cache."""
+    import numpy as np
+    import torch
+    from cuda.bindings import driver as cu
+
+    torch.empty(1, device="cuda")  # make the primary context current
+    nx, ny, nz = len(x), len(y), len(z)
+    V = nx * ny * nz
+    allocs = []
+
+    def dev_in(arr):
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        d = _check(cu.cuMemAlloc(max(4, a.nbytes)), "cuMemAlloc")
+        allocs.append(d)
+        _check(cu.cuMemcpyHtoD(d, a.ctypes.data, a.nbytes), "cuMemcpyHtoD")
+        return _DevPtr(d)
+
+    def dev_out(n):
+        d = _check(cu.cuMemAlloc(4 * n), "cuMemAlloc")
+        allocs.append(d)
+        return _DevPtr(d)
+
+    try:
+        p_r, p_i = dev_out(V), dev_out(V)
+        args = [dev_in(a) for a in (x, y, z, ant, meas_r, meas_i, rxo)]
+        cuda_image(p_r, p_i, *args, slope, wavelength, fft_spacing, nx, ny, nz, num_ant, num_rx,
+                   samples, is_ti, interp)
+        out_r = np.empty(V, np.float32)
+        out_i = np.empty(V, np.float32)
+        _check(cu.cuMemcpyDtoH(out_r.ctypes.data, p_r.ptr, 4 * V), "cuMemcpyDtoH")
+        _check(cu.cuMemcpyDtoH(out_i.ctypes.data, p_i.ptr, 4 * V), "cuMemcpyDtoH")
+    finally:
+        for d in allocs:
+            cu.cuMemFree(d)
+    return out_r, out_i

@@ -1,0 +1,60 @@
+"""The uneven 24-object batch (config 4: seeds 0-23, grids 32^3-96^3, apertures 32^2-96^2
+at 2-4 mm pitch, 64-256 frequencies, 500-5000 points on a box, sphere or cylinder, 10-25
+dB) in one persistent launch with the autotuner's work granularity, recorded in a CUDA
+graph and replayed: every object against its individually launched result, and against
+the FP64 oracle on a seeded 512-voxel subset of its grid (relative L2 of image and vote,
+median normal angle over the subset's masked voxels)."""
+import numpy as np
+import pytest
+
+from mmnorm_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+TOL = 2e-5
+
+
+def test_config4_batch_vs_individual_and_oracle(cuda_dev, oracle):
+    import torch
+    from mmnorm_b200 import autotune, ops
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=cuda_dev)
+    scs = scenes.config4_objects(sign=-1, device=cuda_dev)
+    assert len(scs) == 24
+    objs = [dict(x_locs=t(sc.x_locs), y_locs=t(sc.y_locs), z_locs=t(sc.z_locs),
+                 antenna_locs=t(sc.antenna_locs), rx_offsets=t(np.zeros((1, 3), np.float32)),
+                 meas=t(sc.meas), wavelength=sc.wavelength, slope=sc.slope) for sc in scs]
+    tuned = autotune.tune_batched(objs)
+    plan = ops.BatchPlan(objs, items_per_slot=tuned["best"])
+    plan.capture()
+    for _ in range(2):  # two replays: the second must not depend on the first's leftovers
+        plan.replay()
+    torch.cuda.synchronize()
+    worst_ind, worst_orc, worst_ang = 0.0, 0.0, 0.0
+    for o, (sc, (img, vote)) in enumerate(zip(scs, plan.results())):
+        si, sv = ops.backproject(*(objs[o][k] for k in ("x_locs", "y_locs", "z_locs",
+                                                        "antenna_locs", "rx_offsets", "meas")),
+                                 sc.wavelength, sc.slope)
+        torch.cuda.synchronize()
+        rel = lambda a, b: float((a - b).abs().norm() / b.abs().norm())
+        e_img, e_vote = rel(img, si), rel(vote, sv)
+        worst_ind = max(worst_ind, e_img, e_vote)
+        assert e_img < TOL and e_vote < TOL, (sc.name, e_img, e_vote)
+        rng = np.random.default_rng(o)
+        idx = np.sort(rng.choice(sc.num_voxels, 512, replace=False))
+        Io, Wo = oracle.full(sc.voxel_centres(idx), sc.antenna_locs, np.zeros((1, 3)), sc.meas,
+                             sc.wavelength, sc.slope, phase_mode=1)
+        I = img.reshape(-1).cpu().numpy()
+        W = vote.reshape(3, -1).cpu().numpy().T
+        e_io, e_wo = oracle.rel_l2(I[idx], Io), oracle.rel_l2(W[idx], Wo)
+        worst_orc = max(worst_orc, e_io, e_wo)
+        assert e_io < TOL and e_wo < TOL, (sc.name, e_io, e_wo)
+        sel = np.abs(Io) > 0.05 * np.abs(I).max()
+        if sel.sum():
+            _, _, raw_o = oracle.normals_from_vote(Io, Wo, 0.0)
+            _, _, raw = oracle.normals_from_vote(I[idx].astype(np.complex128),
+                                                 W[idx].astype(np.complex128), 0.0)
+            med = float(np.median(oracle.angle_deg(raw[sel], raw_o[sel])))
+            worst_ang = max(worst_ang, med)
+            assert med < 0.5, (sc.name, med)
+    print("config 4: worst rel-L2 vs individual %.2e, vs FP64 oracle %.2e, worst median "
+          "normal angle %.2e deg" % (worst_ind, worst_orc, worst_ang))

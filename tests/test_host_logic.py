@@ -1,6 +1,8 @@
 """Host-side logic of the drop-in wrappers against the oracle's restatement of the
-reference wrappers, and the synthetic scene generator.  CPU only."""
+reference wrappers, and the synthetic scene generator.  CPU only except the normal
+epilogue, which runs on the device."""
 import numpy as np
+import pytest
 
 from mmnorm_b200 import py_image_gpu, py_sn_est_gpu, scenes
 
@@ -57,18 +59,28 @@ def test_mask_coordinates_follow_reference_meshgrid_order():
     np.testing.assert_array_equal(coords, full[filt])
 
 
-def test_raw_normals_from_vote_matches_oracle(oracle):
+@pytest.mark.gpu
+def test_raw_normals_from_vote_matches_oracle(cuda_dev, oracle):
+    """The drop-in's normal epilogue (formed on the device, masked on the host in the
+    image's dtype) against the oracle's restatement of py_sn_est_gpu.py:326-376."""
     rng = np.random.default_rng(4)
     shape = (3, 4, 5)
     V = 60
     I = (rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64)
     W = (rng.standard_normal((3, V)) + 1j * rng.standard_normal((3, V))).astype(np.complex64)
-    out = py_sn_est_gpu.raw_normals_from_vote(I.reshape(shape), W.reshape((3,) + shape), 0.2)
-    unit, mask, raw = oracle.normals_from_vote(I.astype(np.complex128),
-                                               W.T.astype(np.complex128), 0.2)
-    got = out.reshape(V, 3)
-    assert np.array_equal(np.isnan(got[:, 0]), ~mask)
-    np.testing.assert_allclose(got[mask], raw[mask], rtol=1e-6)
+    for image in (I, I.astype(np.complex128)):
+        out = py_sn_est_gpu.raw_normals_from_vote(image.reshape(shape), W.reshape((3,) + shape),
+                                                  0.2)
+        unit, mask, raw = oracle.normals_from_vote(I.astype(np.complex128),
+                                                   W.T.astype(np.complex128), 0.2)
+        got = out.reshape(V, 3)
+        assert out.dtype == np.float64
+        assert np.array_equal(np.isnan(got[:, 0]), ~mask)
+        err = np.linalg.norm(got[mask] - raw[mask], axis=1)
+        assert np.all(err <= 2e-6 * np.linalg.norm(raw[mask], axis=1))
+        out_u = py_sn_est_gpu.raw_normals_from_vote(image.reshape(shape),
+                                                    W.reshape((3,) + shape), 0.2, unit=True)
+        np.testing.assert_allclose(out_u.reshape(V, 3)[mask], unit[mask], atol=2e-6)
 
 
 def test_scene_configs_have_baseline_shapes():
