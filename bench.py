@@ -492,7 +492,7 @@ def ours_arm(args):
                               "normals with NaN, phase centres; wall clock, one call"}
 
     interp = None
-    if rank == 0 and world == 1 and not args.no_interp and args.aperture == 128:
+    if rank == 0 and world == 1 and not args.no_interp:
         interp = time_interp(dev, sc)
     reference_cuda = None
     if rank == 0 and world == 1 and not args.no_reference_cuda and args.aperture == 128:

@@ -162,12 +162,16 @@ def test_fast_native_path_image_and_vote(cuda_dev, oracle, R, ti, grid, n_ap):
     img_e, vote_e = _backproject(d, "interp")
     assert _rel(img_f, img_e) < TOL
     assert _rel(vote_f, vote_e) < TOL
+    # against the FP64 oracle (the reference's FP32 path, FP64 phasor and sums) the bit-exact
+    # form carries the reference's FP32 accumulation error (~4e-5 here); the fast form may
+    # add no more than its phasor error to it
     sc = d["sc"]
     Io, Wo = oracle.interp(sc.voxel_centres(), d["ant_np"], d["rxo_np"], d["fft_np"],
                            float(d["wl"]), float(d["fsp"]), is_ti=bool(ti), dist_mode=1,
                            vote=True)
-    assert _rel(img_f, Io) < TOL
-    assert _rel(vote_f, Wo.T) < TOL
+    assert _rel(img_e, Io) < 5e-4
+    assert _rel(img_f, Io) < _rel(img_e, Io) + TOL
+    assert _rel(vote_f, Wo.T) < _rel(vote_e, Wo.T) + TOL
 
 
 def test_fast_out_of_range_and_launch_extent(cuda_dev):
