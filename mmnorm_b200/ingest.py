@@ -31,9 +31,13 @@ def _device():
 
 
 def unpack_adc(raw_bytes, device=None):
-    """complex64 [N, 4] device tensor from the bytes of one 77 GHz .bin file."""
+    """complex64 [N, 4] device tensor from the bytes of one 77 GHz .bin file.  A file that
+    is not whole rows of 8 int16 values is refused with ValueError, as the reference's
+    reshape refuses it (generic_loader.py:533)."""
     dev = device or _device()
     raw = np.frombuffer(raw_bytes, dtype="<i2")
+    if raw.size % 8:
+        raise ValueError("77 GHz ADC data of %d int16 values is not whole rows of 8" % raw.size)
     n = raw.size // 8
     src = torch.as_tensor(raw[: n * 8].copy(), device=dev)
     out = torch.empty((n, 4), dtype=torch.complex64, device=dev)

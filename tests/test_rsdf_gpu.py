@@ -71,3 +71,21 @@ def test_rsdf_one_large_component(cuda_dev):
     assert len(valid) == 1 and not np.isnan(out).any()
     ref = RO.rsdf(n, RO.coords(x, x, x), labeled, valid, x)
     np.testing.assert_array_equal(out, ref)
+
+
+def test_rsdf_matches_reference_fixture(cuda_dev):
+    """Against outputs of the reference's own sdf._find_connected_components and
+    sdf._construct_rsdf_components (tests/golden/make_golden_next.py; cc3d's partition
+    from scipy): the same labels, valid components and RSDF values, bit for bit."""
+    from conftest import load_golden
+    from mmnorm_b200 import rsdf
+    g = load_golden("rsdf_ref")
+    for c in range(int(g["cases"])):
+        p = "c%d_" % c
+        out, labeled, valid, _ = rsdf.compute_rsdf(g[p + "normals"], g[p + "x"], g[p + "y"],
+                                                   g[p + "z"])
+        np.testing.assert_array_equal(labeled, g[p + "labeled"])
+        np.testing.assert_array_equal(valid, g[p + "valid"])
+        ref = g[p + "rsdf"]
+        np.testing.assert_array_equal(np.isnan(out), np.isnan(ref))
+        np.testing.assert_array_equal(out[~np.isnan(ref)], ref[~np.isnan(ref)])

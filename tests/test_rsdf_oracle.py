@@ -40,3 +40,21 @@ def test_components_partition():
     # labels numbered by first voxel in C order
     firsts = [np.flatnonzero(lab.ravel() == k)[0] for k in range(2, lab.max() + 1)]
     assert firsts == sorted(firsts)
+
+
+def test_restatement_matches_reference_fixture():
+    """The restatement against outputs of the reference's own functions
+    (tests/golden/make_golden_next.py): labels, valid components, RSDF bit for bit."""
+    from conftest import load_golden
+    g = load_golden("rsdf_ref")
+    for c in range(int(g["cases"])):
+        p = "c%d_" % c
+        normals, x, y, z = g[p + "normals"], g[p + "x"], g[p + "y"], g[p + "z"]
+        lab, mask = RO.components(normals)
+        np.testing.assert_array_equal(lab, g[p + "labeled"])
+        valid = RO.valid_labels(lab, mask, x)
+        np.testing.assert_array_equal(valid, g[p + "valid"])
+        out = RO.rsdf(normals, RO.coords(x, y, z), lab, valid, x)
+        ref = g[p + "rsdf"]
+        np.testing.assert_array_equal(np.isnan(out), np.isnan(ref))
+        np.testing.assert_array_equal(out[~np.isnan(ref)], ref[~np.isnan(ref)])
