@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip the reference CUDA kernel's full matched filter")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-next-rows", action="store_true",
+                    help="skip the isosurface-channel and RSDF legs")
     ap.add_argument("--variant", default=None,
                     help="force a mixed kernel variant by name instead of autotuning")
     ap.add_argument("--aperture", type=int, default=128,
@@ -497,6 +499,9 @@ def ours_arm(args):
     reference_cuda = None
     if rank == 0 and world == 1 and not args.no_reference_cuda and args.aperture == 128:
         reference_cuda = time_reference_cuda_full(dev, sc)
+    next_rows = None
+    if rank == 0 and world == 1 and not args.no_next_rows:
+        next_rows = time_next_rows(dev)
     accuracy = None
     if acc_mixed is not None:
         accuracy = accuracy_report(dev, sc, acc_idx, acc_mixed[0],
@@ -600,6 +605,7 @@ def ours_arm(args):
             "interp": interp,
             "reference_cuda": reference_cuda,
             "accuracy": accuracy,
+            "next_rows": next_rows,
         }
         line.update(out)
         print(json.dumps(line))
@@ -991,6 +997,95 @@ def time_interp(dev, sc, nbins=4096):
     else:
         out["reference"] = "unavailable: reference cubins not built"
     return out
+
+
+def time_next_rows(dev):
+    """The steps after the normals, each beside the reference's own path on the same GPU
+    or host: (1) isosurface channel simulation at the reference's ray settings (2048 x 2048
+    rays, 80 degree fields of view, 512 wavelengths over 77.5-80.5 GHz, TI offset) on a
+    200 x 220 x 120 grid at 1 mm holding the RSDF of a 4 cm sphere on a +-8 mm shell, 8
+    antennas, against the reference's ray-marching extension (built from source) plus the
+    torch steps of _simulate_channels (isosurface_optimization.py:116-208); (2) the RSDF of
+    a 3-voxel spherical cap on a 64^3 grid against the sequential breadth-first search of
+    sdf.py:122-224 (the restatement pinned to the reference's outputs), and on a 128^3 grid.
+    Host wall clock, synchronised, after a warm-up."""
+    import torch
+    from mmnorm_b200 import isosurface, rsdf
+    from oracle import iso_oracle as IO
+    from oracle import rsdf_oracle as RO
+    C = 2.99792458e8
+    out = {}
+    vs = 0.001
+    x = -0.05 + vs * np.arange(200)
+    y = -0.06 + vs * np.arange(220)
+    z = -0.40 + vs * np.arange(120)
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    r = np.sqrt((X - 0.05) ** 2 + (Y - 0.05) ** 2 + (Z + 0.33) ** 2) - 0.04
+    sdf = np.where(np.abs(r) < 0.008, r, -50.0).astype(np.float32)[..., None]
+    bbox = [x[0], y[0], z[0], x[-1], y[-1], z[-1]]
+    wl = C / np.arange(77.5e9, 80.5e9, 3e9 / 512)
+    rng = np.random.default_rng(0)
+    A = 8
+    loc = np.stack([rng.uniform(0.0, 0.1, A), rng.uniform(0.0, 0.1, A), np.zeros(A)], 1)
+    dirs = np.tile(np.array([[0, 0, 1.0]], np.float32), (A, 1))
+    W = H = 2048
+    fov = 80.0
+    scene = isosurface.make_scene(sdf, bbox, vs, wl, W, H, fov, fov, True)
+    taus = torch.zeros((1, 1))
+    ch = None
+
+    def ours():
+        nonlocal ch
+        ch = isosurface.simulate_channels_batch(scene, taus, loc, dirs)
+
+    t_ours = min(_wall_ms(ours, reps=3))
+    iso = {"grid": list(sdf.shape[:3]), "rays": W * H, "antennas": A, "wavelengths": len(wl),
+           "ours_ms": t_ours}
+    if IO.available():
+        grid = torch.as_tensor(sdf, device=dev)
+        wl_t = torch.as_tensor(wl, device=dev)
+        refs = []
+
+        def ref():
+            refs.clear()
+            for a in range(A):
+                refs.append(IO.simulate_channels(bbox, vs, W, H, fov, fov, grid,
+                                                 torch.as_tensor(loc[a]), dirs[a], wl_t,
+                                                 torch.zeros(1), True))
+
+        iso["reference_ms"] = min(_wall_ms(ref, reps=2))
+        iso["speedup"] = iso["reference_ms"] / t_ours
+        iso["max_rel_l2"] = max(float((ch[0, a] - refs[a]).abs().norm() / refs[a].abs().norm())
+                                for a in range(A))
+        iso["reference"] = "ray_tracing.cpp + ray_tracing_kernel.cu built from source, torch steps"
+    else:
+        iso["reference"] = "unavailable: reference ray-marching extension not built"
+    out["isosurface"] = iso
+    for n in (64, 128):
+        c = (n - 1) / 2
+        g = np.indices((n, n, n)).astype(np.float64)
+        rr = np.sqrt(((g - c) ** 2).sum(0))
+        shell = (rr > n * 0.35) & (rr < n * 0.35 + 3) & (g[2] < c + n * 0.1)
+        nrm = np.stack([(g[k] - c) / np.maximum(rr, 1e-9) for k in range(3)], -1)
+        nrm[~shell] = np.nan
+        xs = np.arange(n) * 0.002
+        res = {}
+
+        def ours_rsdf():
+            res["out"] = rsdf.compute_rsdf(nrm, xs, xs, xs)
+
+        rec = {"voxels_in_mask": int(shell.sum()), "ours_ms": min(_wall_ms(ours_rsdf, reps=2))}
+        if n == 64:
+            out_g, lab, valid, _ = res["out"]
+            t0 = time.perf_counter()
+            ref = RO.rsdf(nrm, RO.coords(xs, xs, xs), lab, valid, xs)
+            rec["sequential_search_ms"] = 1e3 * (time.perf_counter() - t0)
+            rec["speedup"] = rec["sequential_search_ms"] / rec["ours_ms"]
+            rec["bit_identical"] = bool(np.array_equal(np.nan_to_num(ref, nan=7.0),
+                                                       np.nan_to_num(out_g, nan=7.0)))
+        out["rsdf_cap%d" % n] = rec
+    return out
+
 
 
 def accuracy_report(dev, sc, idx, sub_mixed, sub_plain, max_mixed, max_plain):

@@ -50,6 +50,12 @@ constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im
 // on the wrapped angle.
 constexpr int kAnchorPoly = 0;
 constexpr int kAnchorFixed = 1;
+// kAnchorFixed2: the fixed-point anchors of kAnchorFixed with a cheaper prologue -- the
+// FP64 range from an FP32 rsqrt seed and one Newton step, the per-sample turn count
+// u = -d slope/c as 64-bit fixed point from the FP64 rounding constant (no 64-bit
+// conversion), the rotation z from u's top word (integer quarter turns + FP32 Taylor),
+// the block step as u << 5 and the start phase rounded to 2^-33 turns.
+constexpr int kAnchorFixed2 = 2;
 
 // One work item: voxel tile `tile` of p against antenna split `split`.  The two stage
 // buffers' mbarriers are initialised by the caller; `gchunk` counts the chunks this CTA
@@ -128,15 +134,28 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
 #pragma unroll
                 for (int k = 0; k < T; ++k) {
                     const double x = vx[k], y = vy[k], z = vz[k];
-                    d0[k] = range_fp64(x, y, z, a0r, mono, p.ti);
-                    d1[k] = range_fp64(x, y, z, a1r, mono, p.ti);
-                    cis_fp64_phase_pair(-d0[k] * p.kd, -d1[k] * p.kd, zr[k], zi[k], nzi[k]);
                     c2r[k] = c2i[k] = make_float2(0.f, 0.f);
-                    if constexpr (ANCHOR == kAnchorFixed) {
-                        ph0[k] = turns_to_fixed(-d0[k] * p.t0);
-                        ph1[k] = turns_to_fixed(-d1[k] * p.t0);
-                        st0[k] = turns_to_fixed(-d0[k] * p.tblk);
-                        st1[k] = turns_to_fixed(-d1[k] * p.tblk);
+                    if constexpr (ANCHOR == kAnchorFixed2) {
+                        d0[k] = range_fp64_newton(x, y, z, a0r, mono, p.ti);
+                        d1[k] = range_fp64_newton(x, y, z, a1r, mono, p.ti);
+                        const unsigned long long u0 = turns_fixed64(-d0[k] * p.tsmp);
+                        const unsigned long long u1 = turns_fixed64(-d1[k] * p.tsmp);
+                        cis_turns_pair((int32_t)(u0 >> 32), (int32_t)(u1 >> 32), zr[k], zi[k],
+                                       nzi[k]);
+                        st0[k] = u0 << 5;
+                        st1[k] = u1 << 5;
+                        ph0[k] = turns_fixed_top(-d0[k] * p.t0);
+                        ph1[k] = turns_fixed_top(-d1[k] * p.t0);
+                    } else {
+                        d0[k] = range_fp64(x, y, z, a0r, mono, p.ti);
+                        d1[k] = range_fp64(x, y, z, a1r, mono, p.ti);
+                        cis_fp64_phase_pair(-d0[k] * p.kd, -d1[k] * p.kd, zr[k], zi[k], nzi[k]);
+                        if constexpr (ANCHOR == kAnchorFixed) {
+                            ph0[k] = turns_to_fixed(-d0[k] * p.t0);
+                            ph1[k] = turns_to_fixed(-d1[k] * p.t0);
+                            st0[k] = turns_to_fixed(-d0[k] * p.tblk);
+                            st1[k] = turns_to_fixed(-d1[k] * p.tblk);
+                        }
                     }
                 }
                 for (int b = 0; b < nblk; ++b) {
@@ -163,7 +182,7 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
                         float2 anr, ani, nani;
-                        if constexpr (ANCHOR == kAnchorFixed) {
+                        if constexpr (ANCHOR != kAnchorPoly) {
                             fixed_cis(ph0[k], anr.x, ani.x);
                             fixed_cis(ph1[k], anr.y, ani.y);
                             nani = make_float2(-ani.x, -ani.y);
@@ -208,18 +227,38 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
                 double d[T];
                 unsigned long long ph[T], stp[T];
                 float2 zr[P], zi[P], nzi[P], c2r[P], c2i[P];
+                if constexpr (ANCHOR == kAnchorFixed2) {
+                    int32_t za[T];
 #pragma unroll
-                for (int k = 0; k < T; ++k) {
-                    d[k] = range_fp64((double)vx[k], (double)vy[k], (double)vz[k], ar, mono, p.ti);
-                    if constexpr (ANCHOR == kAnchorFixed) {
-                        ph[k] = turns_to_fixed(-d[k] * p.t0);
-                        stp[k] = turns_to_fixed(-d[k] * p.tblk);
+                    for (int k = 0; k < T; ++k) {
+                        d[k] = range_fp64_newton((double)vx[k], (double)vy[k], (double)vz[k], ar,
+                                                 mono, p.ti);
+                        const unsigned long long u = turns_fixed64(-d[k] * p.tsmp);
+                        za[k] = (int32_t)(u >> 32);
+                        stp[k] = u << 5;
+                        ph[k] = turns_fixed_top(-d[k] * p.t0);
                     }
-                }
 #pragma unroll
-                for (int q = 0; q < P; ++q) {
-                    cis_fp64_phase_pair(-d[2 * q] * p.kd, -d[2 * q + 1] * p.kd, zr[q], zi[q], nzi[q]);
-                    c2r[q] = c2i[q] = make_float2(0.f, 0.f);
+                    for (int q = 0; q < P; ++q) {
+                        cis_turns_pair(za[2 * q], za[2 * q + 1], zr[q], zi[q], nzi[q]);
+                        c2r[q] = c2i[q] = make_float2(0.f, 0.f);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        d[k] = range_fp64((double)vx[k], (double)vy[k], (double)vz[k], ar, mono,
+                                          p.ti);
+                        if constexpr (ANCHOR == kAnchorFixed) {
+                            ph[k] = turns_to_fixed(-d[k] * p.t0);
+                            stp[k] = turns_to_fixed(-d[k] * p.tblk);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < P; ++q) {
+                        cis_fp64_phase_pair(-d[2 * q] * p.kd, -d[2 * q + 1] * p.kd, zr[q], zi[q],
+                                            nzi[q]);
+                        c2r[q] = c2i[q] = make_float2(0.f, 0.f);
+                    }
                 }
                 for (int b = 0; b < nblk; ++b) {
                     const float4 *mb = m4 + b * kBlockF;
@@ -245,7 +284,7 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
 #pragma unroll
                     for (int q = 0; q < P; ++q) {
                         float2 anr, ani, nani;
-                        if constexpr (ANCHOR == kAnchorFixed) {
+                        if constexpr (ANCHOR != kAnchorPoly) {
                             fixed_cis(ph[2 * q], anr.x, ani.x);
                             fixed_cis(ph[2 * q + 1], anr.y, ani.y);
                             nani = make_float2(-ani.x, -ani.y);
@@ -523,6 +562,12 @@ const FwdVariant *fwd_variants(int *count) {
     // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
         {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed>()},
+        // the cheaper prologue (kAnchorFixed2)
+        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n128_s24", 1, pers_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), 24 * 1024},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed2>()},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n256_s24", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed2>(), 24 * 1024},
+        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed2>(), "mixed_antpair_fx2_t1_n256", 2, pers_ptr<1, 256, kFormMixedAntPair, kAnchorFixed2>()},
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair, kAnchorFixed2>(), "mixed_antpair_fx2_t2_n256", 2, pers_ptr<2, 256, kFormMixedAntPair, kAnchorFixed2>()},
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t2_n256", 2, pers_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>()},
         {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t1_n256", 2, pers_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>()},
         {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t4_n128", 1, pers_ptr<4, 128, kFormMixedPair, kAnchorFixed>()},

@@ -21,6 +21,7 @@ struct FwdParams {
     const int32_t *mono_flag; // device word: 1 when all RX offsets are zero
     double k0, kd;         // 2*pi/lambda, 2*pi*slope/c
     double t0, tblk;       // 1/lambda and 32*slope/c: turns per metre of range
+    double tsmp;           // slope/c: turns per metre of range per sample
     double ti;             // 0.15 or 0
     int32_t num_tiles;
     int32_t num_splits;

@@ -178,6 +178,7 @@ int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
     fp.kd = 2.0 * kPi * p->slope / kC;
     fp.t0 = 1.0 / p->wavelength;
     fp.tblk = (double)kBlockF * p->slope / kC;
+    fp.tsmp = p->slope / kC;
     fp.ti = p->is_ti_radar ? 0.15 : 0.0;
     fp.num_tiles = pl.tiles;
     fp.num_splits = pl.splits;
@@ -1018,6 +1019,7 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     f.kd = 2.0 * kPi * p->slope / kC;
     f.t0 = 1.0 / p->wavelength;
     f.tblk = (double)kBlockF * p->slope / kC;
+    f.tsmp = p->slope / kC;
     f.ti = p->is_ti_radar ? 0.15 : 0.0;
     f.num_tiles = pl.tiles;
     f.num_splits = pl.splits;
@@ -1396,6 +1398,7 @@ extern "C" int mmn_batch_upload(mmn_batch *b, void *workspace, size_t workspace_
         f.kd = 2.0 * kPi * p.slope / kC;
         f.t0 = 1.0 / p.wavelength;
         f.tblk = (double)kBlockF * p.slope / kC;
+        f.tsmp = p.slope / kC;
         f.ti = p.is_ti_radar ? 0.15 : 0.0;
         f.num_tiles = ob.tiles;
         f.num_splits = std::max(1, ob.splits);

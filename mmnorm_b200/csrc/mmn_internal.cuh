@@ -129,6 +129,89 @@ __device__ __forceinline__ double range_fp64(double vx, double vy, double vz,
     return d + ti;
 }
 
+// ---------------------------------------------------------------------------------
+// Cheaper forms of the per-(voxel, antenna) prologue (the "fx2" anchor family).
+// ---------------------------------------------------------------------------------
+
+// sqrt(r2) in FP64 from an FP32 reciprocal-square-root seed and one Newton step
+// s' = s + (r2 - s^2) / (2 s), s = r2 * y: the seed's ~2^-22 relative error squares to
+// ~1e-13 (a femtometre at a metre of range).  r2 below 1e-30 (a voxel on the antenna)
+// gives a value below 2e-15 instead of 0.
+__device__ __forceinline__ double sqrt_newton(double r2) {
+    const double y = (double)rsqrtf(fmaxf((float)r2, 1e-30f));
+    const double s = r2 * y;
+    return fma(fma(-s, s, r2), 0.5 * y, s);
+}
+
+__device__ __forceinline__ double range_fp64_newton(double vx, double vy, double vz,
+                                                    const AntRec &a, bool mono, double ti) {
+    const double dx = vx - a.tx[0], dy = vy - a.tx[1], dz = vz - a.tx[2];
+    const double f = sqrt_newton(fma(dx, dx, fma(dy, dy, dz * dz)));
+    double d;
+    if (mono) {
+        d = f + f;
+    } else {
+        const double bx = vx - a.rx[0], by = vy - a.rx[1], bz = vz - a.rx[2];
+        d = f + sqrt_newton(fma(bx, bx, fma(by, by, bz * bz)));
+    }
+    return d + ti;
+}
+
+// w turns as 32.32 fixed point (the top word = the wrapped turn count in 2^-32 steps),
+// from the 1.5*2^52 rounding constant instead of a 64-bit conversion: a = w*2^32 is
+// exact, (a + M) - M = rint(a) whose low word IS the top word, and the exact remainder
+// a - rint(a), scaled by 2^32 and rounded the same way, is the low word (signed).
+// Valid for |w| < 2^19 turns.
+__device__ __forceinline__ unsigned long long turns_fixed64(double w) {
+    const double kM = 6755399441055744.0;  // 1.5 * 2^52
+    const double a = w * 4294967296.0;
+    const double t1 = a + kM;
+    const double r = a - (t1 - kM);
+    const double t2 = fma(r, 4294967296.0, kM);
+    const unsigned long long hi = (unsigned int)__double2loint(t1);
+    const long long lo = __double2loint(t2);
+    return (hi << 32) + (unsigned long long)lo;
+}
+
+// The same with the low word zero (a start phase rounded to 2^-33 turns).
+__device__ __forceinline__ unsigned long long turns_fixed_top(double w) {
+    const double kM = 6755399441055744.0;
+    return (unsigned long long)(unsigned int)__double2loint(fma(w, 4294967296.0, kM)) << 32;
+}
+
+// (cos, sin) of two angles given as wrapped 2^-32-turn integers: the nearest quarter turn
+// q from the top bits, the remainder r in [-2^29, 2^29) (an angle in [-pi/4, pi/4)) in
+// FP32, the Taylor polynomials of cis_fp64_phase_pair, rotated by q quarter turns.
+__device__ __forceinline__ void cis_turns_pair(int32_t a0, int32_t a1, float2 &c, float2 &s,
+                                               float2 &ns) {
+    const uint32_t q0 = ((uint32_t)a0 + 0x20000000u) >> 30;
+    const uint32_t q1 = ((uint32_t)a1 + 0x20000000u) >> 30;
+    const int32_t r0 = (int32_t)((uint32_t)a0 - (q0 << 30));
+    const int32_t r1 = (int32_t)((uint32_t)a1 - (q1 << 30));
+    const float kTurn = 1.46291807926715968e-9f;  // 2*pi / 2^32
+    const float2 x = make_float2((float)r0 * kTurn, (float)r1 * kTurn);
+    const float2 x2 = __fmul2_rn(x, x);
+    const float2 x3 = __fmul2_rn(x2, x);
+    float2 sp = __ffma2_rn(x2, make_float2(2.75573192239858906526e-6f, 2.75573192239858906526e-6f),
+                           make_float2(-1.98412698412698412698e-4f, -1.98412698412698412698e-4f));
+    sp = __ffma2_rn(x2, sp, make_float2(8.33333333333333333333e-3f, 8.33333333333333333333e-3f));
+    sp = __ffma2_rn(x2, sp, make_float2(-1.66666666666666666667e-1f, -1.66666666666666666667e-1f));
+    sp = __ffma2_rn(x3, sp, x);
+    float2 cp = __ffma2_rn(x2, make_float2(-2.75573192239858906526e-7f, -2.75573192239858906526e-7f),
+                           make_float2(2.48015873015873015873e-5f, 2.48015873015873015873e-5f));
+    cp = __ffma2_rn(x2, cp, make_float2(-1.38888888888888888889e-3f, -1.38888888888888888889e-3f));
+    cp = __ffma2_rn(x2, cp, make_float2(4.16666666666666666667e-2f, 4.16666666666666666667e-2f));
+    cp = __ffma2_rn(x2, cp, make_float2(-0.5f, -0.5f));
+    cp = __ffma2_rn(x2, cp, make_float2(1.0f, 1.0f));
+    float s0 = (q0 & 1) ? cp.x : sp.x, c0 = (q0 & 1) ? -sp.x : cp.x;
+    float s1 = (q1 & 1) ? cp.y : sp.y, c1 = (q1 & 1) ? -sp.y : cp.y;
+    if (q0 & 2) { s0 = -s0; c0 = -c0; }
+    if (q1 & 2) { s1 = -s1; c1 = -c1; }
+    c = make_float2(c0, c1);
+    s = make_float2(s0, s1);
+    ns = make_float2(-s0, -s1);
+}
+
 // ---------------------------------------------------------------- status / errors
 __device__ __forceinline__ void set_status(int32_t *status, int32_t code) {
     if (status) atomicCAS(status, 0, code);

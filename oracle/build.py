@@ -19,7 +19,9 @@ Two things are built here, both as checkers, never as the product:
        sm_100a with torch's extension builder, imported by ``oracle/iso_oracle.py``.
 
 Outputs under ``oracle/_ref`` and ``oracle/_build`` are git-ignored build products.
-Usage: ``python oracle/build.py [--ref-root PATH]``.
+Usage: ``python oracle/build.py [--ref-root PATH]``; the mmNorm checkout comes from
+``--ref-root`` or the ``MMNORM_REF_ROOT`` environment variable, and without either only
+the C oracle is built.
 """
 from __future__ import annotations
 
@@ -31,7 +33,6 @@ import sysconfig
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF_ROOT = "/root/reference"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
@@ -58,10 +59,13 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
-def build_ref(ref_root: str = DEFAULT_REF_ROOT, force: bool = False) -> dict:
-    """Compile the reference's imager and kernels; returns {name: path} of what exists."""
+def build_ref(ref_root: str | None = None, force: bool = False) -> dict:
+    """Compile the reference's imager and kernels from the checkout at `ref_root` (default:
+    $MMNORM_REF_ROOT); returns {name: path} of what exists.  Without a checkout nothing is
+    built."""
     built = {}
-    if not os.path.isdir(ref_root):
+    ref_root = ref_root or os.environ.get("MMNORM_REF_ROOT")
+    if not ref_root or not os.path.isdir(ref_root):
         return built
     os.makedirs(REF_OUT, exist_ok=True)
     cpp_dir = os.path.join(ref_root, "src", "data_processing", "cpp")
@@ -113,7 +117,7 @@ def build_ref(ref_root: str = DEFAULT_REF_ROOT, force: bool = False) -> dict:
 
 
 def main(argv: list[str]) -> int:
-    ref_root = DEFAULT_REF_ROOT
+    ref_root = None
     if "--ref-root" in argv:
         ref_root = argv[argv.index("--ref-root") + 1]
     force = "--force" in argv

@@ -147,7 +147,7 @@ def test_deterministic_and_status_clean(cuda_dev):
     assert ops.read_status(ws) == 0
 
 
-@pytest.mark.parametrize("idx", list(range(16)))
+@pytest.mark.parametrize("idx", list(range(24)))
 def test_every_mixed_variant(cuda_dev, oracle, idx):
     from mmnorm_b200 import ops
     n = len(ops.variants("mixed"))
@@ -228,7 +228,9 @@ def test_pair_and_scalar_mixed_forms_agree_bitwise(cuda_dev, n_ap):
     groups = [("mixed_ffma_t4_n128", "mixed_ffma2_t4_n128", "mixed_antpair_t2_n256",
                "mixed_antpair_t1_n256"),
               ("mixed_ffma2_fx_t2_n256", "mixed_ffma2_fx_t4_n128", "mixed_antpair_fx_t2_n256",
-               "mixed_antpair_fx_t1_n256")]
+               "mixed_antpair_fx_t1_n256"),
+              ("mixed_ffma2_fx2_t2_n256", "mixed_ffma2_fx2_t2_n128_s24", "mixed_antpair_fx2_t2_n256",
+               "mixed_antpair_fx2_t1_n256")]
     sc = scenes.sphere_scene(seed=16, n_ap=n_ap, nf=64, n_vox=11, n_pts=20)
     for group in groups:
         out = []
@@ -253,5 +255,47 @@ def test_autotuner_selects_a_variant(cuda_dev):
     try:
         assert res["best"] in range(len(ops.variants("mixed")))
         assert len(res["times_ms"]) == len(ops.variants("mixed"))
+    finally:
+        ops.set_variant("mixed", 0)
+
+
+@pytest.mark.parametrize("idx", list(range(24)))
+def test_every_mixed_variant_edge_cases(cuda_dev, oracle, idx):
+    """Each mixed variant on F = 1, 33 and 100 (not multiples of the 32-sample block), on
+    several RX offsets with the TI offset and a ragged antenna count, and with per-antenna
+    position offsets, against the FP64 oracle."""
+    from mmnorm_b200 import ops
+    n = len(ops.variants("mixed"))
+    if idx >= n:
+        pytest.skip("no variant %d" % idx)
+    rng = np.random.default_rng(30 + idx)
+    ops.set_variant("mixed", idx)
+    try:
+        for nf in (1, 33, 100):
+            sc = small_scene(seed=40 + nf, nf=max(nf, 2), n_vox=7)
+            meas = sc.meas[:, :nf]
+            I, W = run_ops(cuda_dev, sc, "mixed", meas=meas)
+            Io, Wo = oracle.full(sc.voxel_centres(), sc.antenna_locs, np.zeros((1, 3)), meas,
+                                 sc.wavelength, sc.slope)
+            assert oracle.rel_l2(I, Io) < TOL_MIXED, nf
+            assert oracle.rel_l2(W, Wo) < TOL_MIXED, nf
+        sc = small_scene(seed=5)
+        rxo = np.array([[0, -0.005, 0], [0, -0.007, 0.001], [0.002, 0, 0]], np.float32)
+        A = sc.antenna_locs.shape[0]
+        ant = np.repeat(sc.antenna_locs, 3, axis=0)[: A + 7]
+        meas = (rng.standard_normal((ant.shape[0], 40)) +
+                1j * rng.standard_normal((ant.shape[0], 40))).astype(np.complex64)
+        I, W = run_ops(cuda_dev, sc, "mixed", rxo=rxo, ti=True, meas=meas, ant=ant)
+        Io, Wo = oracle.full(sc.voxel_centres(), ant, rxo, meas, sc.wavelength, sc.slope,
+                             is_ti=True)
+        assert oracle.rel_l2(I, Io) < TOL_MIXED
+        assert oracle.rel_l2(W, Wo) < TOL_MIXED
+        pos = rng.normal(0, 5e-4, sc.antenna_locs.shape)
+        I, W = run_ops(cuda_dev, sc, "mixed", pos=pos)
+        moved = (sc.antenna_locs.astype(np.float64) + pos.astype(np.float32)).astype(np.float32)
+        Io, Wo = oracle.full(sc.voxel_centres(), moved, np.zeros((1, 3)), sc.meas,
+                             sc.wavelength, sc.slope)
+        assert oracle.rel_l2(I, Io) < 1e-4
+        assert oracle.rel_l2(W, Wo) < 1e-4
     finally:
         ops.set_variant("mixed", 0)
