@@ -908,10 +908,17 @@ def time_interp(dev, sc, nbins=4096):
            "pairs": pairs}
     exact_ms = _event_ms(lambda: ours(1))
     exact = torch.complex(qr, qi).clone()
-    fast_ms = _event_ms(lambda: ours(2))
-    fast = torch.complex(qr, qi).clone()
     rel = lambda a, b: float((a.to(torch.complex128) - b.to(torch.complex128)).norm() /
                              b.to(torch.complex128).norm())
+    forms = {}
+    for form in ("scalar", "packed_alt_order", "packed"):  # the default form last
+        ops.set_interp_fast_form(form)
+        f_ms = _event_ms(lambda: ours(2))
+        forms[form] = {"ms": min(f_ms),
+                       "rel_l2_vs_exact": rel(torch.complex(qr, qi), exact)}
+    fast_ms = [forms["packed"]["ms"]]
+    fast = torch.complex(qr, qi).clone()
+    out["fast_forms"] = forms
     out["ours_exact_ms"] = min(exact_ms)
     out["ours_fast_ms"] = min(fast_ms)
     out["fast_rel_l2_vs_exact"] = rel(fast, exact)

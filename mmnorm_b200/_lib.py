@@ -100,6 +100,7 @@ SIGNATURES = [
     ("mmn_backproject_nufft", _I, [_PROB, _P, _P, _P, _SZ, _P]),
     ("mmn_set_position_pass", _I, [_I32]),
     ("mmn_set_measurement_pass", _I, [_I32]),
+    ("mmn_set_interp_fast_form", _I, [_I32]),
     ("mmn_num_position_variants", _I, []),
     ("mmn_position_variant_name", ctypes.c_char_p, [_I32]),
     ("mmn_set_position_variant", _I, [_I32]),

@@ -10,9 +10,15 @@
 // through shared memory in chunks instead of being re-read from global memory by
 // every thread, the measurement gather is a single 8-byte load of the complex bin,
 // and the image pass can fuse the vote vector W = sum_i c_i (tx_i + o_i/2 - v).
+#include <atomic>
+
 #include "bp_kernels.cuh"
 
 namespace mmn {
+
+// Form of the fast image pass: 0 packed voxel pairs (default), 1 scalar, 2 packed with the
+// other contraction order of the squared range.
+std::atomic<int> g_interp_fast_form{0};
 
 namespace {
 constexpr int kInterpThreads = 256;
@@ -241,11 +247,11 @@ __device__ __forceinline__ int fast_bin(float path, float fsp, float half_inv) {
     const float h = path * half_inv;
     const float hm = h + kRoundMagic;
     const float r = hm - kRoundMagic;
-    const int above = r > h ? 1 : 0;
-    const float fr = h - (r - (float)above);
+    const bool above = r > h;
+    const float fr = h - (above ? r - 1.f : r);
     const float tol = fmaxf(h, 1.f) * 1.2e-6f;
     if (fr < tol || fr > 1.f - tol) return (int)floorf(path / fsp / 2);
-    return __float_as_int(hm) - __float_as_int(kRoundMagic) - above;
+    return __float_as_int(hm) - __float_as_int(kRoundMagic) - (above ? 1 : 0);
 }
 
 // (cos, sin) of -2 pi path / lambda with 1/lambda = hi + lo.
@@ -437,6 +443,250 @@ __global__ void __launch_bounds__(kInterpThreads) interp_normals_fast_kernel(con
     p.n_z[ind] = acc_z;
 }
 
+// ---------------------------------------------------------------------------------
+// Fast form, packed: each thread's two voxels ride in the two halves of Blackwell's packed
+// FP32 instructions (FADD2 / FMUL2 / FFMA2; each half rounds exactly like the scalar
+// instruction), so the per-pair arithmetic -- differences, squared range, range bin,
+// turn count, complex product, vote -- issues once per voxel pair.  The square roots, the
+// sine/cosine and the gathers stay per voxel.  The squared range must reproduce the
+// reference's FP32 value bit for bit (its path length selects the bin and sets the phase
+// to ~1e-4 rad per ulp), so the FMA contraction order of dx*dx + dy*dy + dz*dz is a
+// template parameter: ORDER 0 = fma(dz, dz, fma(dx, dx, dy*dy)), ORDER 1 =
+// fma(dz, dz, fma(dy, dy, dx*dx)).
+// ---------------------------------------------------------------------------------
+namespace {
+// Staged antenna of the packed form: values pre-negated and duplicated in both halves, so
+// one 16-byte shared load feeds a packed instruction directly.
+struct __align__(16) PackAnt {
+    float2 ntx, nty, ntz, pad0;  // -TX
+    float2 nox, noy, noz, pad1;  // -RX offset
+    float2 ux, uy, uz, pad2;     // TX + o/2 (vote anchor)
+};
+
+__device__ __forceinline__ float2 dup(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ void stage_pack_chunk(const InterpParams &p, int a0, int n,
+                                                 PackAnt *sh) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int i = a0 + j;
+        const int rx = i % p.num_rx;
+        const float tx = p.ant[3 * i + 0], ty = p.ant[3 * i + 1], tz = p.ant[3 * i + 2];
+        const float ox = p.rxo[3 * rx + 0], oy = p.rxo[3 * rx + 1], oz = p.rxo[3 * rx + 2];
+        PackAnt a;
+        a.ntx = dup(-tx);
+        a.nty = dup(-ty);
+        a.ntz = dup(-tz);
+        a.nox = dup(-ox);
+        a.noy = dup(-oy);
+        a.noz = dup(-oz);
+        a.ux = dup(tx + ox / 2);
+        a.uy = dup(ty + oy / 2);
+        a.uz = dup(tz + oz / 2);
+        a.pad0 = a.pad1 = a.pad2 = dup(0.f);
+        sh[j] = a;
+    }
+}
+
+__device__ __forceinline__ bool pack_chunk_has_offsets(const PackAnt *sh, int n) {
+    bool any = false;
+    for (int j = threadIdx.x; j < n; j += blockDim.x)
+        any |= (sh[j].nox.x != 0.f) | (sh[j].noy.x != 0.f) | (sh[j].noz.x != 0.f);
+    return __syncthreads_or(any) != 0;
+}
+
+template <int ORDER>
+__device__ __forceinline__ float2 sumsq2(float2 dx, float2 dy, float2 dz) {
+    if (ORDER == 0) return __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
+    return __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+}
+
+// The two voxels' FP32 path lengths, as imaging_gpu.cu:70-89 forms them.
+template <int ORDER, bool MONO>
+__device__ __forceinline__ float2 path2(float2 vx, float2 vy, float2 vz, const PackAnt &a,
+                                        bool ti) {
+    const float2 dx = __fadd2_rn(vx, a.ntx);
+    const float2 dy = __fadd2_rn(vy, a.nty);
+    const float2 dz = __fadd2_rn(vz, a.ntz);
+    const float2 s = sumsq2<ORDER>(dx, dy, dz);
+    const float2 leg = make_float2(sqrtf(s.x), sqrtf(s.y));
+    float2 path;
+    if (MONO) {
+        path = __fadd2_rn(leg, leg);
+    } else {
+        const float2 bx = __fadd2_rn(dx, a.nox);
+        const float2 by = __fadd2_rn(dy, a.noy);
+        const float2 bz = __fadd2_rn(dz, a.noz);
+        const float2 sb = sumsq2<ORDER>(bx, by, bz);
+        path = __fadd2_rn(leg, make_float2(sqrtf(sb.x), sqrtf(sb.y)));
+    }
+    if (ti) {  // float += double, as the reference adds its 0.15 m
+        path.x += 0.15;
+        path.y += 0.15;
+    }
+    return path;
+}
+
+// fast_bin for two paths (the arithmetic packed, the rare division fallback per voxel).
+__device__ __forceinline__ int2 bin2(float2 path, float fsp, float half_inv) {
+    const float2 h = __fmul2_rn(path, dup(half_inv));
+    const float2 hm = __fadd2_rn(h, dup(kRoundMagic));
+    const float2 r = __fadd2_rn(hm, dup(-kRoundMagic));
+    const bool ax = r.x > h.x, ay = r.y > h.y;
+    const float2 fr = __fadd2_rn(__fadd2_rn(h, make_float2(-r.x, -r.y)),
+                                 make_float2(ax ? 1.f : 0.f, ay ? 1.f : 0.f));
+    const float2 tol = __fmul2_rn(make_float2(fmaxf(h.x, 1.f), fmaxf(h.y, 1.f)), dup(1.2e-6f));
+    int2 b = make_int2(__float_as_int(hm.x) - __float_as_int(kRoundMagic) - (ax ? 1 : 0),
+                       __float_as_int(hm.y) - __float_as_int(kRoundMagic) - (ay ? 1 : 0));
+    if (fr.x < tol.x || fr.x > 1.f - tol.x) b.x = (int)floorf(path.x / fsp / 2);
+    if (fr.y < tol.y || fr.y > 1.f - tol.y) b.y = (int)floorf(path.y / fsp / 2);
+    return b;
+}
+
+// fast_phasor for two paths: returns (cos, sin) of -2 pi path / lambda per half.
+__device__ __forceinline__ void phasor2(float2 path, float hi, float lo, float2 &c,
+                                        float2 &s) {
+    const float2 qn = __fmul2_rn(path, dup(-hi));               // -q
+    const float2 e = __ffma2_rn(path, dup(hi), qn);             // path*hi - q, exact
+    const float2 nn = __fadd2_rn(__fadd2_rn(qn, dup(kRoundMagic)), dup(-kRoundMagic));  // -n
+    const float2 g = __ffma2_rn(nn, dup(-1.f), qn);             // -(q - n), exact
+    const float2 w = __ffma2_rn(path, dup(lo), e);              // path*lo + e
+    const float2 f = __ffma2_rn(g, dup(-1.f), w);               // (q - n) + w
+    const float2 ang = __fmul2_rn(f, dup(-6.28318530717958647692f));
+    __sincosf(ang.x, &s.x, &c.x);
+    __sincosf(ang.y, &s.y, &c.y);
+}
+
+template <int ORDER, bool MONO, bool VOTE, bool SOA>
+__device__ __forceinline__ void pack_image_chunk(const InterpParams &p, const PackAnt *sh,
+                                                 int a0, int n, float range_max, bool ti,
+                                                 float2 vx, float2 vy, float2 vz, float2 nvx,
+                                                 float2 nvy, float2 nvz, float2 (&acc)[8]) {
+#pragma unroll 2
+    for (int j = 0; j < n; ++j) {
+        const PackAnt &a = sh[j];
+        const size_t row = (size_t)(a0 + j) * (size_t)p.nbins;
+        const float2 path = path2<ORDER, MONO>(vx, vy, vz, a, ti);
+        const bool v0 = !(path.x < 0 || path.x > range_max);
+        const bool v1 = !(path.y < 0 || path.y > range_max);
+        int2 b = bin2(path, p.fft_spacing, p.half_inv_fsp);
+        b.x = v0 ? b.x : 0;
+        b.y = v1 ? b.y : 0;
+        float2 mre, mim;
+        if (SOA) {
+            mre = make_float2(__ldg(p.meas_r + row + b.x), __ldg(p.meas_r + row + b.y));
+            mim = make_float2(__ldg(p.meas_i + row + b.x), __ldg(p.meas_i + row + b.y));
+        } else {
+            const float2 m0 = __ldg(p.meas + row + b.x), m1 = __ldg(p.meas + row + b.y);
+            mre = make_float2(m0.x, m1.x);
+            mim = make_float2(m0.y, m1.y);
+        }
+        float2 c, s;
+        phasor2(path, p.inv_lambda_hi, p.inv_lambda_lo, c, s);
+        float2 re = __ffma2_rn(mre, c, __fmul2_rn(mim, make_float2(-s.x, -s.y)));
+        float2 im = __ffma2_rn(mre, s, __fmul2_rn(mim, c));
+        re = make_float2(v0 ? re.x : 0.f, v1 ? re.y : 0.f);
+        im = make_float2(v0 ? im.x : 0.f, v1 ? im.y : 0.f);
+        acc[0] = __fadd2_rn(acc[0], re);
+        acc[1] = __fadd2_rn(acc[1], im);
+        if (VOTE) {
+            const float2 ex = __fadd2_rn(a.ux, nvx);
+            const float2 ey = __fadd2_rn(a.uy, nvy);
+            const float2 ez = __fadd2_rn(a.uz, nvz);
+            acc[2] = __ffma2_rn(re, ex, acc[2]);
+            acc[3] = __ffma2_rn(im, ex, acc[3]);
+            acc[4] = __ffma2_rn(re, ey, acc[4]);
+            acc[5] = __ffma2_rn(im, ey, acc[5]);
+            acc[6] = __ffma2_rn(re, ez, acc[6]);
+            acc[7] = __ffma2_rn(im, ez, acc[7]);
+        }
+    }
+}
+
+template <int ORDER, bool VOTE, bool SOA>
+__device__ __forceinline__ void pack_image_dispatch(const InterpParams &p, const PackAnt *sh,
+                                                    int a0, int n, float range_max, bool ti,
+                                                    bool offsets, float2 vx, float2 vy,
+                                                    float2 vz, float2 nvx, float2 nvy,
+                                                    float2 nvz, float2 (&acc)[8]) {
+    if (offsets)
+        pack_image_chunk<ORDER, false, VOTE, SOA>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
+                                                  nvy, nvz, acc);
+    else
+        pack_image_chunk<ORDER, true, VOTE, SOA>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
+                                                 nvy, nvz, acc);
+}
+}  // namespace
+
+// Image pass in packed fast form: voxels rel and rel + blockDim of each 2*blockDim tile
+// (coalesced stores), optionally fusing the vote vector.
+template <int ORDER>
+__global__ void __launch_bounds__(kInterpThreads) interp_image_pack_kernel(const InterpParams p) {
+    __shared__ PackAnt sh[kInterpChunk];
+    const int64_t nyz = (int64_t)p.ny * p.nz;
+    const float range_max = p.fft_spacing * p.nbins;
+    const bool ti = p.is_ti != 0;
+    int64_t vox[2];
+    bool active[2];
+    float px[2], py[2], pz[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int64_t rel = ((int64_t)blockIdx.x * 2 + k) * blockDim.x + threadIdx.x;
+        active[k] = rel < p.count && rel + p.start < p.nvox;
+        const int64_t v = active[k] ? rel + p.start : 0;
+        vox[k] = v;
+        const int x = (int)(v / nyz);
+        const int y = (int)((v - (int64_t)x * nyz) / p.nz);
+        const int z = (int)(v - (int64_t)x * nyz - (int64_t)y * p.nz);
+        px[k] = p.x_locs[x];
+        py[k] = p.y_locs[y];
+        pz[k] = p.z_locs[z];
+    }
+    const float2 vx = make_float2(px[0], px[1]), vy = make_float2(py[0], py[1]),
+                 vz = make_float2(pz[0], pz[1]);
+    const float2 nvx = make_float2(-px[0], -px[1]), nvy = make_float2(-py[0], -py[1]),
+                 nvz = make_float2(-pz[0], -pz[1]);
+    float2 acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = dup(0.f);
+    const bool soa = p.meas == nullptr;
+    for (int a0 = 0; a0 < p.num_ant; a0 += kInterpChunk) {
+        const int n = min(kInterpChunk, p.num_ant - a0);
+        __syncthreads();
+        stage_pack_chunk(p, a0, n, sh);
+        __syncthreads();
+        const bool offsets = pack_chunk_has_offsets(sh, n);
+        if (p.vote) {
+            if (soa) pack_image_dispatch<ORDER, true, true>(p, sh, a0, n, range_max, ti, offsets,
+                                                            vx, vy, vz, nvx, nvy, nvz, acc);
+            else pack_image_dispatch<ORDER, true, false>(p, sh, a0, n, range_max, ti, offsets,
+                                                         vx, vy, vz, nvx, nvy, nvz, acc);
+        } else {
+            if (soa) pack_image_dispatch<ORDER, false, true>(p, sh, a0, n, range_max, ti,
+                                                             offsets, vx, vy, vz, nvx, nvy, nvz,
+                                                             acc);
+            else pack_image_dispatch<ORDER, false, false>(p, sh, a0, n, range_max, ti, offsets,
+                                                          vx, vy, vz, nvx, nvy, nvz, acc);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (!active[k]) continue;
+        const int64_t v = vox[k];
+        const float re = k ? acc[0].y : acc[0].x, im = k ? acc[1].y : acc[1].x;
+        if (p.out_r) {
+            p.out_r[v] = re;
+            p.out_i[v] = im;
+        }
+        if (p.image) p.image[v] = make_float2(re, im);
+        if (p.vote) {
+            p.vote[v] = make_float2(k ? acc[2].y : acc[2].x, k ? acc[3].y : acc[3].x);
+            p.vote[p.nvox + v] = make_float2(k ? acc[4].y : acc[4].x, k ? acc[5].y : acc[5].x);
+            p.vote[2 * p.nvox + v] = make_float2(k ? acc[6].y : acc[6].x,
+                                                 k ? acc[7].y : acc[7].x);
+        }
+    }
+}
+
 cudaError_t launch_interp_image(const InterpParams &p, cudaStream_t stream) {
     if (p.count <= 0) return cudaSuccess;
     const int64_t blocks = (p.count + kInterpThreads - 1) / kInterpThreads;
@@ -453,9 +703,18 @@ cudaError_t launch_interp_normals(const InterpParams &p, cudaStream_t stream) {
 
 cudaError_t launch_interp_image_fast(const InterpParams &p, cudaStream_t stream) {
     if (p.count <= 0) return cudaSuccess;
-    const int64_t per = (int64_t)kInterpThreads * kFastT;
+    const int64_t per = (int64_t)kInterpThreads * 2;  // kFastT == 2 in every form
     const int64_t blocks = (p.count + per - 1) / per;
-    interp_image_fast_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+    switch (g_interp_fast_form.load()) {
+    case 1:
+        interp_image_fast_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+        break;
+    case 2:
+        interp_image_pack_kernel<1><<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+        break;
+    default:
+        interp_image_pack_kernel<0><<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+    }
     return cudaGetLastError();
 }
 

@@ -1,6 +1,8 @@
 // bp_kernels.cuh -- kernel parameter blocks and launch helpers shared by the
 // kernel files and the C ABI (capi.cu).
 #pragma once
+#include <atomic>
+
 #include "mmn_internal.cuh"
 
 namespace mmn {
@@ -171,6 +173,7 @@ cudaError_t launch_interp_normals(const InterpParams &p, cudaStream_t stream);
 // fast form of both passes: same path length and range bin as the reference, the
 // phasor from a wrapped FP32 turn count and the hardware sine/cosine
 cudaError_t launch_interp_image_fast(const InterpParams &p, cudaStream_t stream);
+extern std::atomic<int> g_interp_fast_form;  // form of the fast image pass (bp_interp.cu)
 cudaError_t launch_interp_normals_fast(const InterpParams &p, cudaStream_t stream);
 
 // --------------------------------------------------------------------- epilogue

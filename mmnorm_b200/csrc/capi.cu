@@ -948,6 +948,12 @@ extern "C" int mmn_backproject_nufft(const mmn_problem *p, float *image, float *
     return MMN_OK;
 }
 
+extern "C" int mmn_set_interp_fast_form(int32_t form) {
+    if (form < 0 || form > 2) return MMN_ERR_INVALID_ARGUMENT;
+    g_interp_fast_form.store(form);
+    return MMN_OK;
+}
+
 extern "C" int mmn_set_measurement_pass(int32_t form) {
     if (form != MMN_PASS_INTERP && form != MMN_PASS_HORNER) return MMN_ERR_INVALID_ARGUMENT;
     g_meas_form.store(form);

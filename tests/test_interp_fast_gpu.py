@@ -84,8 +84,9 @@ def _cuda_image(d, flag, start=0, count=-1, dev=None):
     return out_r.cpu().numpy() + 1j * out_i.cpu().numpy()
 
 
+@pytest.mark.parametrize("fast_form", FORMS, indirect=True)
 @pytest.mark.parametrize("R,ti", [(1, False), (4, True)])
-def test_fast_image_vs_reference_kernel(cuda_dev, R, ti):
+def test_fast_image_vs_reference_kernel(cuda_dev, R, ti, fast_form):
     import torch
     from oracle import ref_cuda
     if not ref_cuda.available():
@@ -151,12 +152,25 @@ def test_fast_sn_est_vs_reference_kernel(cuda_dev, R):
     assert _rel(f, r) < TOL
 
 
+FORMS = ["packed", "scalar", "packed_alt_order"]
+
+
+@pytest.fixture
+def fast_form(request):
+    from mmnorm_b200 import ops
+    ops.set_interp_fast_form(request.param)
+    yield request.param
+    ops.set_interp_fast_form("packed")
+
+
+@pytest.mark.parametrize("fast_form", FORMS, indirect=True)
 @pytest.mark.parametrize("R,ti,grid,n_ap", [(1, False, None, 12), (2, True, (7, 9, 11), 18),
                                             (1, True, (5, 3, 37), 17)])
-def test_fast_native_path_image_and_vote(cuda_dev, oracle, R, ti, grid, n_ap):
+def test_fast_native_path_image_and_vote(cuda_dev, oracle, R, ti, grid, n_ap, fast_form):
     """Ragged grids (voxel counts not a multiple of the 512 voxels of a CTA), antenna counts
     across the 256-antenna staging chunk (18^2 * 2 = 648, 17^2 = 289), several RX offsets
-    and the TI offset: fused image and vote vs the bit-exact kernel and the FP64 oracle."""
+    and the TI offset: fused image and vote vs the bit-exact kernel and the FP64 oracle,
+    for every form of the fast image pass."""
     d = _setup(cuda_dev, R=R, ti=ti, grid=grid, n_ap=n_ap)
     img_f, vote_f = _backproject(d, "interp_fast")
     img_e, vote_e = _backproject(d, "interp")
@@ -248,9 +262,12 @@ def test_fast_dropin_wrappers(cuda_dev):
     np.testing.assert_allclose(np.linalg.norm(unit[ok], axis=-1), 1, rtol=1e-6)
 
 
-def test_fast_at_the_full_workload(cuda_dev):
+@pytest.mark.parametrize("fast_form", FORMS, indirect=True)
+def test_fast_at_the_full_workload(cuda_dev, fast_form):
     """128^3 voxels, 128x128 antennas, a 4096-bin range FFT of the 256-sample workload:
-    fast image and vote within 1e-5 of the bit-exact kernel."""
+    fast image and vote within 1e-5 of the bit-exact kernel, for every form of the fast
+    image pass (a squared range one ulp off the reference's moves the phase by ~1e-4 rad,
+    so a form whose FMA order differs from the reference's shows here)."""
     import torch
     from mmnorm_b200 import ops
     sc = scenes.config1(sign=-1, device=cuda_dev)
@@ -269,5 +286,6 @@ def test_fast_at_the_full_workload(cuda_dev):
     rel = lambda a, b: float((a.to(torch.complex128) - b.to(torch.complex128)).norm() /
                              b.to(torch.complex128).norm())
     e_img, e_vote = rel(img_f, img_e), rel(vote_f, vote_e)
-    print("fast vs bit-exact at the workload: image %.2e vote %.2e" % (e_img, e_vote))
+    print("fast (%s) vs bit-exact at the workload: image %.2e vote %.2e"
+          % (fast_form, e_img, e_vote))
     assert e_img < TOL_WORKLOAD and e_vote < TOL_WORKLOAD
