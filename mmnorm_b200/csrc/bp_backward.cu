@@ -110,12 +110,13 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_kernel(const BwdParams bp) {
     const bool mono = *p.mono_flag != 0;
     const int nblk = fp / kBlockF;
 
+    int c_failed = -1;  // chunk whose wait gave up; the drain runs after the loop
     for (int c = 0; c < n_chunks; ++c) {
         const int s = c & 1;
         bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
         if (!__syncthreads_and(ok)) {
-            st.drain_after_timeout((uint32_t)c, c + 1 < n_chunks, p.status);
-            return;
+            c_failed = c;
+            break;
         }
         const AntRec *ants = st.ants(s);
         const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
@@ -224,6 +225,10 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_kernel(const BwdParams bp) {
         __syncthreads();
         if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
     }
+    if (c_failed >= 0) {
+        st.drain_after_timeout((uint32_t)c_failed, c_failed + 1 < n_chunks, p.status);
+        return;
+    }
 }
 
 __global__ void bwd_pos_reduce_kernel(const BwdParams bp) {
@@ -285,12 +290,13 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_img_kernel(const BwdParams bp) 
     const bool mono = *p.mono_flag != 0;
     const int nblk = fp / kBlockF;
 
+    int c_failed = -1;  // chunk whose wait gave up; the drain runs after the loop
     for (int c = 0; c < n_chunks; ++c) {
         const int s = c & 1;
         bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
         if (!__syncthreads_and(ok)) {
-            st.drain_after_timeout((uint32_t)c, c + 1 < n_chunks, p.status);
-            return;
+            c_failed = c;
+            break;
         }
         const AntRec *ants = st.ants(s);
         const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
@@ -391,6 +397,10 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_img_kernel(const BwdParams bp) 
         }
         __syncthreads();
         if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
+    }
+    if (c_failed >= 0) {
+        st.drain_after_timeout((uint32_t)c_failed, c_failed + 1 < n_chunks, p.status);
+        return;
     }
 }
 

@@ -60,11 +60,13 @@ constexpr int kAnchorFixed2 = 2;
 // One work item: voxel tile `tile` of p against antenna split `split`.  The two stage
 // buffers' mbarriers are initialised by the caller; `gchunk` counts the chunks this CTA
 // has consumed so far (stage = gchunk & 1, phase parity = (gchunk >> 1) & 1), so a
-// persistent CTA can run item after item on the same barriers.  Returns false if a
-// bounded wait gave up (the status word is set).
+// persistent CTA can run item after item on the same barriers.  Returns -1, or, if a
+// bounded wait gave up (the status word is set), 2 * (global chunk index) + (1 if the
+// next chunk's copy was issued): the caller then drains the stages (drain_stages) after
+// its own loop, which keeps that path out of the loops' register allocation.
 template <int T, int NT, int FORM, int ANCHOR, bool PERSISTENT>
-__device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split,
-                                         unsigned char *smem, uint32_t &gchunk) {
+__device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
+                                        unsigned char *smem, uint32_t &gchunk) {
     static_assert(FORM != kFormMixedPair || T % 2 == 0, "pair form needs an even T");
     Stage st;
     st.bars = reinterpret_cast<uint64_t *>(smem);
@@ -109,13 +111,14 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
     const bool mono = *p.mono_flag != 0;
     const int nblk = fp / kBlockF;
 
+    int c_failed = -1;  // chunk whose wait gave up; the drain runs after the loop
     for (int c = 0; c < n_chunks; ++c) {
         const uint32_t gc = g0 + (uint32_t)c;
         const int s = (int)(gc & 1);
         bool ok = mbar_wait_bounded(&st.bars[s], (gc >> 1) & 1, p.status);
         if (!__syncthreads_and(ok)) {
-            st.drain_after_timeout(gc, c + 1 < n_chunks, p.status);
-            return false;
+            c_failed = c;
+            break;
         }
         const AntRec *ants = st.ants(s);
         const unsigned char *mstage = st.meas(s);
@@ -407,11 +410,13 @@ __device__ __forceinline__ bool fwd_item(const FwdParams &p, int tile, int split
         __syncthreads();
         if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, (int)((g0 + (uint32_t)c) & 1), a_begin, a_end);
     }
+    if (c_failed >= 0)
+        return 2 * (int)(g0 + (uint32_t)c_failed) + (c_failed + 1 < n_chunks ? 1 : 0);
     if (PERSISTENT) gchunk = g0 + (uint32_t)n_chunks;
 
 #pragma unroll
     for (int k = 0; k < T; ++k) store_voxel(p, split, rbase + (int64_t)k * NT, acc[k]);
-    return true;
+    return -1;
 }
 
 __device__ __forceinline__ void init_stage_barriers(unsigned char *smem) {
@@ -429,8 +434,12 @@ template <int T, int NT, int FORM, int ANCHOR = kAnchorPoly>
 __global__ void __launch_bounds__(NT) bp_fwd_kernel(const FwdParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint32_t gchunk = 0;
-    fwd_item<T, NT, FORM, ANCHOR, false>(p, blockIdx.x % p.num_tiles, blockIdx.x / p.num_tiles,
-                                         smem, gchunk);
+    const int failed = fwd_item<T, NT, FORM, ANCHOR, false>(p, blockIdx.x % p.num_tiles,
+                                                             blockIdx.x / p.num_tiles, smem,
+                                                             gchunk);
+    if (failed >= 0)
+        drain_stages(reinterpret_cast<uint64_t *>(smem), (uint32_t)failed >> 1, failed & 1,
+                     p.status);
 }
 
 // Persistent launch over a work list of (object, voxel tile, antenna split) items: every
@@ -442,6 +451,8 @@ __global__ void __launch_bounds__(NT) bp_fwd_persistent(const BatchParams bp) {
     __shared__ int s_item;
     init_stage_barriers(smem);
     uint32_t gchunk = 0;
+    int failed = -1;
+    int32_t *status = nullptr;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(bp.counter, 1);
         __syncthreads();
@@ -452,8 +463,15 @@ __global__ void __launch_bounds__(NT) bp_fwd_persistent(const BatchParams bp) {
         // the item's object parameters as a local copy: read once, then kept in registers
         // (a reference into global memory would be re-read inside the loops)
         const FwdParams obj = bp.objs[w.x];
-        if (!fwd_item<T, NT, FORM, ANCHOR, true>(obj, w.y, w.z, smem, gchunk)) break;
+        failed = fwd_item<T, NT, FORM, ANCHOR, true>(obj, w.y, w.z, smem, gchunk);
+        if (failed >= 0) {
+            status = obj.status;
+            break;
+        }
     }
+    if (failed >= 0)
+        drain_stages(reinterpret_cast<uint64_t *>(smem), (uint32_t)failed >> 1, failed & 1,
+                     status);
 }
 
 __global__ void bp_reduce_partials(const FwdParams p) {

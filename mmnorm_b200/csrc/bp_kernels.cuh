@@ -135,8 +135,8 @@ const char *bwd_pos_nufft_variant_name(int variant);  // null for a bad index
 cudaError_t launch_nufft_tables(int F, int N, int J0, double *sc, double2 *tw,
                                 cudaStream_t stream);
 cudaError_t launch_nufft_grid(const float *meas, int A, int F, int N, int J0, double k0,
-                              double kd, const double *sc, const double2 *tw, float4 *rows,
-                              cudaStream_t stream);
+                              double kd, const double *sc, const double2 *tw, void *rows,
+                              bool fwd_only, cudaStream_t stream);
 
 // ---------------------------------------------------------- interpolated mode
 struct InterpParams {

@@ -155,10 +155,13 @@ __global__ void nufft_tables_kernel(int F, int N, int J0, double *__restrict__ s
 }
 
 // rows[a][jj] = (G'_k.re, G_k.re, G'_k.im, G_k.im) for cell k = (jj - (W/2 - 1)) mod N,
-// jj < N + W - 1: a tap run starting at any cell reads W consecutive entries.
+// jj < N + W - 1: a tap run starting at any cell reads W consecutive entries.  FWD_ONLY:
+// the forward reads only G, so its rows are (G_k.re, G_k.im) -- 8 bytes a cell -- and the
+// G' sums are not formed.
+template <bool FWD_ONLY>
 __global__ void nufft_grid_kernel(const float2 *__restrict__ meas, int F, int N, int J0, int row,
                                   double k0, double kd, const double *__restrict__ sc,
-                                  const double2 *__restrict__ tw, float4 *__restrict__ rows,
+                                  const double2 *__restrict__ tw, void *__restrict__ rows,
                                   int blocks_per_row) {
     const int a = blockIdx.x / blocks_per_row;
     const int jj = (blockIdx.x - a * blocks_per_row) * blockDim.x + threadIdx.x;
@@ -173,15 +176,21 @@ __global__ void nufft_grid_kernel(const float2 *__restrict__ meas, int F, int N,
         const double2 t = __ldg(tw + idx);
         const double ar = s * (double)mv.x, ai = s * (double)mv.y;
         const double pr = fma(ar, t.x, -ai * t.y), pi = fma(ar, t.y, ai * t.x);
-        const double kap = fma((double)j, kd, k0);
         gr += pr;
         gi += pi;
-        hr = fma(kap, pr, hr);
-        hi = fma(kap, pi, hi);
+        if (!FWD_ONLY) {
+            const double kap = fma((double)j, kd, k0);
+            hr = fma(kap, pr, hr);
+            hi = fma(kap, pi, hi);
+        }
         idx += k;
         if (idx >= N) idx -= N;
     }
-    rows[(size_t)a * row + jj] = make_float4((float)hr, (float)gr, (float)hi, (float)gi);
+    if (FWD_ONLY)
+        static_cast<float2 *>(rows)[(size_t)a * row + jj] = make_float2((float)gr, (float)gi);
+    else
+        static_cast<float4 *>(rows)[(size_t)a * row + jj] =
+            make_float4((float)hr, (float)gr, (float)hi, (float)gi);
 }
 
 // Position pass, interpolation form.  VOTE: the loss has a vote term (grad_vote set).
@@ -239,12 +248,13 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_nufft_kernel(const BwdParams bp
     }
     const bool mono = *p.mono_flag != 0;
 
+    int c_failed = -1;  // chunk whose wait gave up; the drain runs after the loop
     for (int c = 0; c < n_chunks; ++c) {
         const int s = c & 1;
         bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
         if (!__syncthreads_and(ok)) {
-            st.drain_after_timeout((uint32_t)c, c + 1 < n_chunks, p.status);
-            return;
+            c_failed = c;
+            break;
         }
         const AntRec *ants = st.ants(s);
         const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
@@ -315,6 +325,10 @@ __global__ void __launch_bounds__(NT) bp_bwd_pos_nufft_kernel(const BwdParams bp
         __syncthreads();
         if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
     }
+    if (c_failed >= 0) {
+        st.drain_after_timeout((uint32_t)c_failed, c_failed + 1 < n_chunks, p.status);
+        return;
+    }
 }
 
 // Launch shapes (voxels per thread, threads per CTA, cap on one shared-memory stage).
@@ -352,7 +366,7 @@ __global__ void __launch_bounds__(NT) bp_fwd_nufft_kernel(const BwdParams bp) {
     st.bars = reinterpret_cast<uint64_t *>(smem);
     st.base = smem + 128;
     st.nas = p.ant_per_stage;
-    st.esz = 16;
+    st.esz = 8;    // (G.re, G.im) cells
     st.fp = p.fp;  // grid row length N + W - 1
     st.stage_bytes = (size_t)st.nas * sizeof(AntRec) + (size_t)st.nas * st.fp * st.esz;
     const int row_len = p.fp;
@@ -390,20 +404,21 @@ __global__ void __launch_bounds__(NT) bp_fwd_nufft_kernel(const BwdParams bp) {
     }
     const bool mono = *p.mono_flag != 0;
 
+    int c_failed = -1;  // chunk whose wait gave up; the drain runs after the loop
     for (int c = 0; c < n_chunks; ++c) {
         const int s = c & 1;
         bool ok = mbar_wait_bounded(&st.bars[s], (uint32_t)((c >> 1) & 1), p.status);
         if (!__syncthreads_and(ok)) {
-            st.drain_after_timeout((uint32_t)c, c + 1 < n_chunks, p.status);
-            return;
+            c_failed = c;
+            break;
         }
         const AntRec *ants = st.ants(s);
-        const float4 *mstage = reinterpret_cast<const float4 *>(st.meas(s));
+        const float2 *mstage = reinterpret_cast<const float2 *>(st.meas(s));
         const int a0 = a_begin + c * st.nas;
         const int na = min(st.nas, a_end - a0);
         for (int a = 0; a < na; ++a) {
             const AntRec &ar = ants[a];
-            const float4 *row = mstage + (size_t)a * row_len;
+            const float2 *row = mstage + (size_t)a * row_len;
             const float txf[3] = {(float)ar.tx[0], (float)ar.tx[1], (float)ar.tx[2]};
             const float rxf[3] = {(float)ar.rx[0], (float)ar.rx[1], (float)ar.rx[2]};
 #pragma unroll
@@ -413,10 +428,8 @@ __global__ void __launch_bounds__(NT) bp_fwd_nufft_kernel(const BwdParams bp) {
                            uq, n, g);
                 float2 h = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int i = 0; i < kNuW; ++i) {
-                    const float4 e = row[g.ix + i];
-                    h = __ffma2_rn(make_float2(g.w[i], g.w[i]), make_float2(e.y, e.w), h);
-                }
+                for (int i = 0; i < kNuW; ++i)
+                    h = __ffma2_rn(make_float2(g.w[i], g.w[i]), row[g.ix + i], h);
                 const float2 an = cis_fp64_phase(-g.d * k0c);
                 const float cr = fmaf(an.x, h.x, -an.y * h.y), ci = fmaf(an.x, h.y, an.y * h.x);
                 const float u0 = ar.virt[0] - vx[k], u1 = ar.virt[1] - vy[k],
@@ -433,6 +446,10 @@ __global__ void __launch_bounds__(NT) bp_fwd_nufft_kernel(const BwdParams bp) {
         }
         __syncthreads();
         if (threadIdx.x == 0 && c + 2 < n_chunks) st.issue(p, c + 2, a_begin, a_end);
+    }
+    if (c_failed >= 0) {
+        st.drain_after_timeout((uint32_t)c_failed, c_failed + 1 < n_chunks, p.status);
+        return;
     }
 #pragma unroll
     for (int k = 0; k < T; ++k) store_voxel(p, split, rbase + (int64_t)k * NT, acc[k]);
@@ -657,13 +674,19 @@ cudaError_t launch_nufft_tables(int F, int N, int J0, double *sc, double2 *tw,
 }
 
 cudaError_t launch_nufft_grid(const float *meas, int A, int F, int N, int J0, double k0,
-                              double kd, const double *sc, const double2 *tw, float4 *rows,
-                              cudaStream_t stream) {
+                              double kd, const double *sc, const double2 *tw, void *rows,
+                              bool fwd_only, cudaStream_t stream) {
     const int nt = 256;
     const int row = nufft_row(N);
     const int bpr = (row + nt - 1) / nt;
-    nufft_grid_kernel<<<(unsigned)((int64_t)A * bpr), nt, 0, stream>>>(
-        reinterpret_cast<const float2 *>(meas), F, N, J0, row, k0, kd, sc, tw, rows, bpr);
+    const unsigned grid = (unsigned)((int64_t)A * bpr);
+    const float2 *m = reinterpret_cast<const float2 *>(meas);
+    if (fwd_only)
+        nufft_grid_kernel<true><<<grid, nt, 0, stream>>>(m, F, N, J0, row, k0, kd, sc, tw, rows,
+                                                         bpr);
+    else
+        nufft_grid_kernel<false><<<grid, nt, 0, stream>>>(m, F, N, J0, row, k0, kd, sc, tw, rows,
+                                                          bpr);
     return cudaGetLastError();
 }
 

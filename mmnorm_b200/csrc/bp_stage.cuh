@@ -6,6 +6,21 @@
 
 namespace mmn {
 
+// After a bounded wait on chunk `gc` of a double-buffered stage gave up: the issuing thread
+// gives each stage that may still have a copy outstanding -- chunk gc, and chunk gc+1 when
+// it was issued -- one more bounded wait, so that a copy which is merely late lands before
+// the CTA exits and its shared memory can go to another CTA.  A copy that misses this wait
+// too may still be in flight when the CTA exits.  Called by every thread of the CTA; not
+// inlined, so that the failure path stays out of the kernels' register allocation.
+static __device__ __noinline__ void drain_stages(uint64_t *bars, uint32_t gc, bool next_issued,
+                                                 int32_t *status) {
+    if (threadIdx.x == 0) {
+        mbar_wait_bounded(&bars[gc & 1], (gc >> 1) & 1, status);
+        if (next_issued) mbar_wait_bounded(&bars[(gc + 1) & 1], ((gc + 1) >> 1) & 1, status);
+    }
+    __syncthreads();
+}
+
 // ----------------------------------------------------------- shared-memory stage
 struct Stage {
     uint64_t *bars;
@@ -32,16 +47,9 @@ struct Stage {
         issue(p, c, c & 1, a_begin, a_end);
     }
     // Called by every thread after a bounded wait on chunk `gc` gave up (the status word
-    // is set).  The issuing thread gives each stage that may still have a copy outstanding
-    // -- chunk gc, and chunk gc+1 when it was issued -- one more bounded wait, so that a
-    // copy which is merely late lands before the CTA exits and its shared memory can go
-    // to another CTA.  A copy that misses this wait too may still be in flight at exit.
+    // is set): see drain_stages.
     __device__ void drain_after_timeout(uint32_t gc, bool next_issued, int32_t *status) const {
-        if (threadIdx.x == 0) {
-            mbar_wait_bounded(&bars[gc & 1], (gc >> 1) & 1, status);
-            if (next_issued) mbar_wait_bounded(&bars[(gc + 1) & 1], ((gc + 1) >> 1) & 1, status);
-        }
-        __syncthreads();
+        drain_stages(bars, gc, next_issued, status);
     }
     __device__ const AntRec *ants(int s) const {
         return reinterpret_cast<const AntRec *>(base + s * stage_bytes);

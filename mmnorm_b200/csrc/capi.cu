@@ -816,7 +816,7 @@ int plan_nufft_forward(const mmn_problem *p, NuFwdPlan *pl) {
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     pl->n = 2 * F;
     pl->row = nufft_row(pl->n);
-    const int rec = (int)sizeof(AntRec) + pl->row * 16;
+    const int rec = (int)sizeof(AntRec) + pl->row * 8;  // (G.re, G.im) cells
     if (rec > kMaxStageBytes) return MMN_ERR_TOO_LARGE;
     pl->fn = fwd_nufft_kernel_ptr(&pl->threads, &pl->vpt);
     pl->ant_per_stage = std::max(1, std::min(16, 24 * 1024 / rec));
@@ -856,7 +856,7 @@ int plan_nufft_forward(const mmn_problem *p, NuFwdPlan *pl) {
     pl->off_ant = off;
     off = align_up(off + (size_t)A * sizeof(AntRec));
     pl->off_rows = off;
-    off = align_up(off + (size_t)A * pl->row * 16);
+    off = align_up(off + (size_t)A * pl->row * 8);
     pl->off_tab = off;
     off = align_up(off + (size_t)pl->n * sizeof(double2) + (size_t)F * sizeof(double));
     pl->off_part = off;
@@ -906,8 +906,8 @@ extern "C" int mmn_backproject_nufft(const mmn_problem *p, float *image, float *
     double *sc = reinterpret_cast<double *>(tw + pl.n);
     const double k0 = 2.0 * kPi / p->wavelength, kd = 2.0 * kPi * p->slope / kC;
     if (launch_nufft_tables(F, pl.n, J0, sc, tw, stream) != cudaSuccess) return MMN_ERR_CUDA;
-    if (launch_nufft_grid(p->meas, A, F, pl.n, J0, k0, kd, sc, tw,
-                          reinterpret_cast<float4 *>(ws + pl.off_rows), stream) != cudaSuccess)
+    if (launch_nufft_grid(p->meas, A, F, pl.n, J0, k0, kd, sc, tw, ws + pl.off_rows, true,
+                          stream) != cudaSuccess)
         return MMN_ERR_CUDA;
     BwdParams bq;
     std::memset(&bq, 0, sizeof(bq));
@@ -1050,8 +1050,8 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
         launch_nufft_tables(F, pl.nu_n, J0, sc, tw, stream) != cudaSuccess)
         return MMN_ERR_CUDA;
     if (grad_pos && pl.nufft) {
-        if (launch_nufft_grid(p->meas, A, F, pl.nu_n, J0, f.k0, f.kd, sc, tw,
-                              reinterpret_cast<float4 *>(ws + pl.off_meas), stream) != cudaSuccess)
+        if (launch_nufft_grid(p->meas, A, F, pl.nu_n, J0, f.k0, f.kd, sc, tw, ws + pl.off_meas,
+                              false, stream) != cudaSuccess)
             return MMN_ERR_CUDA;
         BwdParams bq = bp;
         bq.f.fp = pl.row;

@@ -20,6 +20,16 @@ pytestmark = pytest.mark.gpu
 TOL = 2e-6
 TOL_WORKLOAD = 1e-5
 
+FORMS = ["packed", "scalar", "packed_alt_order"]
+
+
+@pytest.fixture
+def fast_form(request):
+    from mmnorm_b200 import ops
+    ops.set_interp_fast_form(request.param)
+    yield request.param
+    ops.set_interp_fast_form("packed")
+
 
 def _rel(a, b):
     a = np.asarray(a, np.complex128).ravel()
@@ -150,17 +160,6 @@ def test_fast_sn_est_vs_reference_kernel(cuda_dev, R):
     f = np.stack([a.cpu().numpy() for a in fast], 1)
     assert np.abs(r).max() > 0
     assert _rel(f, r) < TOL
-
-
-FORMS = ["packed", "scalar", "packed_alt_order"]
-
-
-@pytest.fixture
-def fast_form(request):
-    from mmnorm_b200 import ops
-    ops.set_interp_fast_form(request.param)
-    yield request.param
-    ops.set_interp_fast_form("packed")
 
 
 @pytest.mark.parametrize("fast_form", FORMS, indirect=True)

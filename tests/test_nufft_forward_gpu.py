@@ -63,9 +63,11 @@ def test_antenna_split_path_and_repeatability(cuda_dev, oracle):
 
 
 def test_sample_count_limit(cuda_dev):
+    """The forward stages one antenna's (G.re, G.im) grid row of 2F + 7 cells of 8 bytes
+    per stage at least: F = 3200 does not fit a 48 KB stage."""
     from mmnorm_b200 import _lib, ops
     sc = small_scene(seed=9, nf=2)
-    meas = np.zeros((sc.antenna_locs.shape[0], 1600), np.complex64)
+    meas = np.zeros((sc.antenna_locs.shape[0], 3200), np.complex64)
     with pytest.raises(_lib.MmnError):
         ops.backproject(_t(sc.x_locs, cuda_dev), _t(sc.y_locs, cuda_dev),
                         _t(sc.z_locs, cuda_dev), _t(sc.antenna_locs, cuda_dev),
@@ -128,3 +130,13 @@ def test_near_the_sample_limit_forward_and_adjoint(cuda_dev, oracle):
                                       gW.T.astype(np.complex128))
     assert oracle.rel_l2(gm.cpu().numpy().astype(np.complex128), gm_o) < 2e-5
     assert oracle.rel_l2(gp.cpu().numpy().astype(np.float64), gp_o) < 2e-4
+
+
+def test_forward_near_its_sample_limit(cuda_dev, oracle):
+    """F = 3000: one forward grid row (6007 cells of 8 bytes, 47 KB) fills a stage."""
+    nf = 3000
+    sc = scenes.sphere_scene(seed=13, n_ap=3, nf=nf, n_vox=4, n_pts=8)
+    I, W = run_ops(cuda_dev, sc, "nufft")
+    Io, Wo = oracle.full(sc.voxel_centres(), sc.antenna_locs, np.zeros((1, 3)), sc.meas,
+                         sc.wavelength, sc.slope)
+    assert oracle.rel_l2(I, Io) < TOL_MIXED and oracle.rel_l2(W, Wo) < TOL_MIXED
