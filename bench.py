@@ -583,7 +583,10 @@ def ours_arm(args):
                        "autotune_ms": tuned["times_ms"]},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": FWD_DRAM_BYTES_PER_LAUNCH,
+                         "traffic": FWD_DRAM_BYTES_PER_LAUNCH.get(variant["name"]) if args.aperture == 128
+                         else None,
+                         "traffic_source": "one full-size ncu capture of this variant "
+                                           "(profiles/bp_fwd_kernel_dram_boxcyl128.md)",
                          "kernel": "bp_fwd_kernel " + variant["name"],
                          "flops_per_update": 8,
                          "peak_source": "FP32 FFMA probe (mmn_fp32_peak_probe) timed in this "
@@ -911,7 +914,7 @@ def time_interp(dev, sc, nbins=4096):
     rel = lambda a, b: float((a.to(torch.complex128) - b.to(torch.complex128)).norm() /
                              b.to(torch.complex128).norm())
     forms = {}
-    for form in ("scalar", "packed_alt_order", "packed"):  # the default form last
+    for form in ("scalar", "packed"):  # the default form last
         ops.set_interp_fast_form(form)
         f_ms = _event_ms(lambda: ours(2))
         forms[form] = {"ms": min(f_ms),
@@ -1142,12 +1145,11 @@ def accuracy_report(dev, sc, idx, sub_mixed, sub_plain, max_mixed, max_plain):
 
 
 
-# DRAM bytes (read + write) of one forward launch at the workload, from one ncu capture of
-# the central 32x32-antenna case (dram__bytes_read.sum + dram__bytes_write.sum of
-# bp_fwd_kernel, -c 1) scaled by the antenna count (x16): the staged rows are re-read per
-# CTA, so the traffic grows with the antennas a CTA sweeps.  Capture and scaling are
-# summarised in profiles/bp_fwd_kernel_boxcyl128_ap32.md.
-FWD_DRAM_BYTES_PER_LAUNCH = None
+# DRAM bytes (read + write) of one forward launch at the full workload, by kernel variant:
+# one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum on one full-size launch
+# (a one-pass metric set, checked on the small case first), summarised in
+# profiles/bp_fwd_kernel_dram_boxcyl128.md.  Variants without a capture report null.
+FWD_DRAM_BYTES_PER_LAUNCH = {"mixed_antpair_fx2_t1_n256": 38597632 + 37433856}
 
 
 def main():

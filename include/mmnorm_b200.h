@@ -51,11 +51,9 @@ extern "C" {
  * per term from the reference's phasor.  Bins up to 2^22 (else MMN_ERR_TOO_LARGE). */
 #define MMN_MODE_INTERP_FAST 3
 
-/* Form of the fast interpolated image pass (no reference counterpart), process-wide:
+/* Form of the fast interpolated passes (no reference counterpart), process-wide:
  * 0 (default) two voxels per thread in packed FP32 instructions, 1 the same arithmetic
- * in scalar instructions, 2 packed with the other FMA order of the squared range (kept
- * for checking which order reproduces the reference's FP32 path).  All give the
- * reference's range bins. */
+ * in scalar instructions.  Both give the reference's range bins and path lengths. */
 int mmn_set_interp_fast_form(int32_t form);
 
 /* Problem description.  All array pointers are device pointers. */

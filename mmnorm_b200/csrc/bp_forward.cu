@@ -586,6 +586,12 @@ const FwdVariant *fwd_variants(int *count) {
         {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n256_s24", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed2>(), 24 * 1024},
         {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed2>(), "mixed_antpair_fx2_t1_n256", 2, pers_ptr<1, 256, kFormMixedAntPair, kAnchorFixed2>()},
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair, kAnchorFixed2>(), "mixed_antpair_fx2_t2_n256", 2, pers_ptr<2, 256, kFormMixedAntPair, kAnchorFixed2>()},
+        // smaller stages: more resident CTAs (shared memory limits occupancy otherwise)
+        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n128_s16", 1, pers_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), 16 * 1024},
+        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n128_s12", 1, pers_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), 12 * 1024},
+        {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed2>(), "mixed_antpair_fx2_t1_n256_s24", 2, pers_ptr<1, 256, kFormMixedAntPair, kAnchorFixed2>(), 24 * 1024},
+        {1, 128, false, 8, fwd_ptr<1, 128, kFormMixedAntPair, kAnchorFixed2>(), "mixed_antpair_fx2_t1_n128_s24", 2, pers_ptr<1, 128, kFormMixedAntPair, kAnchorFixed2>(), 24 * 1024},
+        {1, 128, false, 8, fwd_ptr<1, 128, kFormMixedAntPair, kAnchorFixed2>(), "mixed_antpair_fx2_t1_n128_s16", 2, pers_ptr<1, 128, kFormMixedAntPair, kAnchorFixed2>(), 16 * 1024},
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t2_n256", 2, pers_ptr<2, 256, kFormMixedAntPair, kAnchorFixed>()},
         {1, 256, false, 8, fwd_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>(), "mixed_antpair_fx_t1_n256", 2, pers_ptr<1, 256, kFormMixedAntPair, kAnchorFixed>()},
         {4, 128, false, 16, fwd_ptr<4, 128, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t4_n128", 1, pers_ptr<4, 128, kFormMixedPair, kAnchorFixed>()},

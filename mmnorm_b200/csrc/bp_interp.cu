@@ -16,8 +16,7 @@
 
 namespace mmn {
 
-// Form of the fast image pass: 0 packed voxel pairs (default), 1 scalar, 2 packed with the
-// other contraction order of the squared range.
+// Form of the fast passes: 0 packed voxel pairs (default), 1 scalar.
 std::atomic<int> g_interp_fast_form{0};
 
 namespace {
@@ -450,9 +449,10 @@ __global__ void __launch_bounds__(kInterpThreads) interp_normals_fast_kernel(con
 // turn count, complex product, vote -- issues once per voxel pair.  The square roots, the
 // sine/cosine and the gathers stay per voxel.  The squared range must reproduce the
 // reference's FP32 value bit for bit (its path length selects the bin and sets the phase
-// to ~1e-4 rad per ulp), so the FMA contraction order of dx*dx + dy*dy + dz*dz is a
-// template parameter: ORDER 0 = fma(dz, dz, fma(dx, dx, dy*dy)), ORDER 1 =
-// fma(dz, dz, fma(dy, dy, dx*dx)).
+// to ~1e-4 rad per ulp): nvcc contracts the reference's dx*dx + dy*dy + dz*dz into
+// fma(dz, dz, fma(dx, dx, dy*dy)), which sumsq2 repeats.  (Measured: that order gives the
+// bit-exact kernel's bins and phases, 7.5e-7 from it at the 128^3 / 16384-antenna
+// workload; the order fma(dz, dz, fma(dy, dy, dx*dx)) is 2.5e-4 away.)
 // ---------------------------------------------------------------------------------
 namespace {
 // Staged antenna of the packed form: values pre-negated and duplicated in both halves, so
@@ -494,20 +494,18 @@ __device__ __forceinline__ bool pack_chunk_has_offsets(const PackAnt *sh, int n)
     return __syncthreads_or(any) != 0;
 }
 
-template <int ORDER>
 __device__ __forceinline__ float2 sumsq2(float2 dx, float2 dy, float2 dz) {
-    if (ORDER == 0) return __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
-    return __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    return __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
 }
 
 // The two voxels' FP32 path lengths, as imaging_gpu.cu:70-89 forms them.
-template <int ORDER, bool MONO>
+template <bool MONO>
 __device__ __forceinline__ float2 path2(float2 vx, float2 vy, float2 vz, const PackAnt &a,
                                         bool ti) {
     const float2 dx = __fadd2_rn(vx, a.ntx);
     const float2 dy = __fadd2_rn(vy, a.nty);
     const float2 dz = __fadd2_rn(vz, a.ntz);
-    const float2 s = sumsq2<ORDER>(dx, dy, dz);
+    const float2 s = sumsq2(dx, dy, dz);
     const float2 leg = make_float2(sqrtf(s.x), sqrtf(s.y));
     float2 path;
     if (MONO) {
@@ -516,7 +514,7 @@ __device__ __forceinline__ float2 path2(float2 vx, float2 vy, float2 vz, const P
         const float2 bx = __fadd2_rn(dx, a.nox);
         const float2 by = __fadd2_rn(dy, a.noy);
         const float2 bz = __fadd2_rn(dz, a.noz);
-        const float2 sb = sumsq2<ORDER>(bx, by, bz);
+        const float2 sb = sumsq2(bx, by, bz);
         path = __fadd2_rn(leg, make_float2(sqrtf(sb.x), sqrtf(sb.y)));
     }
     if (ti) {  // float += double, as the reference adds its 0.15 m
@@ -556,7 +554,7 @@ __device__ __forceinline__ void phasor2(float2 path, float hi, float lo, float2 
     __sincosf(ang.y, &s.y, &c.y);
 }
 
-template <int ORDER, bool MONO, bool VOTE, bool SOA>
+template <bool MONO, bool VOTE, bool SOA>
 __device__ __forceinline__ void pack_image_chunk(const InterpParams &p, const PackAnt *sh,
                                                  int a0, int n, float range_max, bool ti,
                                                  float2 vx, float2 vy, float2 vz, float2 nvx,
@@ -565,7 +563,7 @@ __device__ __forceinline__ void pack_image_chunk(const InterpParams &p, const Pa
     for (int j = 0; j < n; ++j) {
         const PackAnt &a = sh[j];
         const size_t row = (size_t)(a0 + j) * (size_t)p.nbins;
-        const float2 path = path2<ORDER, MONO>(vx, vy, vz, a, ti);
+        const float2 path = path2<MONO>(vx, vy, vz, a, ti);
         const bool v0 = !(path.x < 0 || path.x > range_max);
         const bool v1 = !(path.y < 0 || path.y > range_max);
         int2 b = bin2(path, p.fft_spacing, p.half_inv_fsp);
@@ -602,24 +600,23 @@ __device__ __forceinline__ void pack_image_chunk(const InterpParams &p, const Pa
     }
 }
 
-template <int ORDER, bool VOTE, bool SOA>
+template <bool VOTE, bool SOA>
 __device__ __forceinline__ void pack_image_dispatch(const InterpParams &p, const PackAnt *sh,
                                                     int a0, int n, float range_max, bool ti,
                                                     bool offsets, float2 vx, float2 vy,
                                                     float2 vz, float2 nvx, float2 nvy,
                                                     float2 nvz, float2 (&acc)[8]) {
     if (offsets)
-        pack_image_chunk<ORDER, false, VOTE, SOA>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
+        pack_image_chunk<false, VOTE, SOA>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
                                                   nvy, nvz, acc);
     else
-        pack_image_chunk<ORDER, true, VOTE, SOA>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
+        pack_image_chunk<true, VOTE, SOA>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
                                                  nvy, nvz, acc);
 }
 }  // namespace
 
 // Image pass in packed fast form: voxels rel and rel + blockDim of each 2*blockDim tile
 // (coalesced stores), optionally fusing the vote vector.
-template <int ORDER>
 __global__ void __launch_bounds__(kInterpThreads) interp_image_pack_kernel(const InterpParams p) {
     __shared__ PackAnt sh[kInterpChunk];
     const int64_t nyz = (int64_t)p.ny * p.nz;
@@ -656,15 +653,15 @@ __global__ void __launch_bounds__(kInterpThreads) interp_image_pack_kernel(const
         __syncthreads();
         const bool offsets = pack_chunk_has_offsets(sh, n);
         if (p.vote) {
-            if (soa) pack_image_dispatch<ORDER, true, true>(p, sh, a0, n, range_max, ti, offsets,
+            if (soa) pack_image_dispatch<true, true>(p, sh, a0, n, range_max, ti, offsets,
                                                             vx, vy, vz, nvx, nvy, nvz, acc);
-            else pack_image_dispatch<ORDER, true, false>(p, sh, a0, n, range_max, ti, offsets,
+            else pack_image_dispatch<true, false>(p, sh, a0, n, range_max, ti, offsets,
                                                          vx, vy, vz, nvx, nvy, nvz, acc);
         } else {
-            if (soa) pack_image_dispatch<ORDER, false, true>(p, sh, a0, n, range_max, ti,
+            if (soa) pack_image_dispatch<false, true>(p, sh, a0, n, range_max, ti,
                                                              offsets, vx, vy, vz, nvx, nvy, nvz,
                                                              acc);
-            else pack_image_dispatch<ORDER, false, false>(p, sh, a0, n, range_max, ti, offsets,
+            else pack_image_dispatch<false, false>(p, sh, a0, n, range_max, ti, offsets,
                                                           vx, vy, vz, nvx, nvy, nvz, acc);
         }
     }
@@ -687,6 +684,112 @@ __global__ void __launch_bounds__(kInterpThreads) interp_image_pack_kernel(const
     }
 }
 
+namespace {
+template <bool MONO, bool SOA>
+__device__ __forceinline__ void pack_normals_chunk(const InterpParams &p, const PackAnt *sh,
+                                                   int a0, int n, float range_max, bool ti,
+                                                   float2 vx, float2 vy, float2 vz, float2 nvx,
+                                                   float2 nvy, float2 nvz, float2 ire,
+                                                   float2 iim, float2 inv_mag,
+                                                   float2 (&acc)[3]) {
+#pragma unroll 2
+    for (int j = 0; j < n; ++j) {
+        const PackAnt &a = sh[j];
+        const size_t row = (size_t)(a0 + j) * (size_t)p.nbins;
+        const float2 path = path2<MONO>(vx, vy, vz, a, ti);
+        const bool v0 = !(path.x < 0 || path.x > range_max);
+        const bool v1 = !(path.y < 0 || path.y > range_max);
+        int2 b = bin2(path, p.fft_spacing, p.half_inv_fsp);
+        b.x = v0 ? b.x : 0;
+        b.y = v1 ? b.y : 0;
+        float2 mre, mim;
+        if (SOA) {
+            mre = make_float2(__ldg(p.meas_r + row + b.x), __ldg(p.meas_r + row + b.y));
+            mim = make_float2(__ldg(p.meas_i + row + b.x), __ldg(p.meas_i + row + b.y));
+        } else {
+            const float2 m0 = __ldg(p.meas + row + b.x), m1 = __ldg(p.meas + row + b.y);
+            mre = make_float2(m0.x, m1.x);
+            mim = make_float2(m0.y, m1.y);
+        }
+        float2 c, s;
+        phasor2(path, p.inv_lambda_hi, p.inv_lambda_lo, c, s);
+        const float2 re = __ffma2_rn(mre, c, __fmul2_rn(mim, make_float2(-s.x, -s.y)));
+        const float2 im = __ffma2_rn(mre, s, __fmul2_rn(mim, c));
+        // weight Re(c conj(I)) / |I| (surface_normal_est.cu:138-139); zero for a skipped pair
+        float2 w = __fmul2_rn(__ffma2_rn(re, ire, __fmul2_rn(im, iim)), inv_mag);
+        w = make_float2(v0 ? w.x : 0.f, v1 ? w.y : 0.f);
+        acc[0] = __ffma2_rn(__fadd2_rn(a.ux, nvx), w, acc[0]);
+        acc[1] = __ffma2_rn(__fadd2_rn(a.uy, nvy), w, acc[1]);
+        acc[2] = __ffma2_rn(__fadd2_rn(a.uz, nvz), w, acc[2]);
+    }
+}
+}  // namespace
+
+// Normal pass in packed fast form over a valid-voxel list: entries ind and ind + blockDim
+// of each 2*blockDim tile per thread.
+__global__ void __launch_bounds__(kInterpThreads) interp_normals_pack_kernel(const InterpParams p) {
+    __shared__ PackAnt sh[kInterpChunk];
+    const float range_max = p.fft_spacing * p.nbins;
+    const bool ti = p.is_ti != 0;
+    int ind[2];
+    bool active[2];
+    float px[2], py[2], pz[2], pr[2], pi[2], pm[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int64_t rel = ((int64_t)blockIdx.x * 2 + k) * blockDim.x + threadIdx.x;
+        const int64_t i64 = rel + p.start;
+        active[k] = rel < p.count && i64 < p.num_valid && i64 >= 0;
+        ind[k] = active[k] ? (int)i64 : 0;
+        int x = 0, y = 0, z = 0;
+        if (active[k]) {
+            x = p.vidx_x[ind[k]];
+            y = p.vidx_y[ind[k]];
+            z = p.vidx_z[ind[k]];
+        }
+        px[k] = p.x_locs[x];
+        py[k] = p.y_locs[y];
+        pz[k] = p.z_locs[z];
+        const int64_t v = ((int64_t)x * p.ny + y) * p.nz + z;
+        pr[k] = active[k] ? p.img_r[v] : 1.f;
+        pi[k] = active[k] ? p.img_i[v] : 0.f;
+        pm[k] = 1.f / sqrtf(pr[k] * pr[k] + pi[k] * pi[k]);
+    }
+    const float2 vx = make_float2(px[0], px[1]), vy = make_float2(py[0], py[1]),
+                 vz = make_float2(pz[0], pz[1]);
+    const float2 nvx = make_float2(-px[0], -px[1]), nvy = make_float2(-py[0], -py[1]),
+                 nvz = make_float2(-pz[0], -pz[1]);
+    const float2 ire = make_float2(pr[0], pr[1]), iim = make_float2(pi[0], pi[1]),
+                 inv_mag = make_float2(pm[0], pm[1]);
+    float2 acc[3] = {dup(0.f), dup(0.f), dup(0.f)};
+    const bool soa = p.meas == nullptr;
+    for (int a0 = 0; a0 < p.num_ant; a0 += kInterpChunk) {
+        const int n = min(kInterpChunk, p.num_ant - a0);
+        __syncthreads();
+        stage_pack_chunk(p, a0, n, sh);
+        __syncthreads();
+        const bool offsets = pack_chunk_has_offsets(sh, n);
+        if (!active[0] && !active[1]) continue;
+        if (offsets) {
+            if (soa) pack_normals_chunk<false, true>(p, sh, a0, n, range_max, ti, vx, vy, vz,
+                                                     nvx, nvy, nvz, ire, iim, inv_mag, acc);
+            else pack_normals_chunk<false, false>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
+                                                  nvy, nvz, ire, iim, inv_mag, acc);
+        } else {
+            if (soa) pack_normals_chunk<true, true>(p, sh, a0, n, range_max, ti, vx, vy, vz,
+                                                    nvx, nvy, nvz, ire, iim, inv_mag, acc);
+            else pack_normals_chunk<true, false>(p, sh, a0, n, range_max, ti, vx, vy, vz, nvx,
+                                                 nvy, nvz, ire, iim, inv_mag, acc);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (!active[k]) continue;
+        p.n_x[ind[k]] = k ? acc[0].y : acc[0].x;
+        p.n_y[ind[k]] = k ? acc[1].y : acc[1].x;
+        p.n_z[ind[k]] = k ? acc[2].y : acc[2].x;
+    }
+}
+
 cudaError_t launch_interp_image(const InterpParams &p, cudaStream_t stream) {
     if (p.count <= 0) return cudaSuccess;
     const int64_t blocks = (p.count + kInterpThreads - 1) / kInterpThreads;
@@ -705,23 +808,23 @@ cudaError_t launch_interp_image_fast(const InterpParams &p, cudaStream_t stream)
     if (p.count <= 0) return cudaSuccess;
     const int64_t per = (int64_t)kInterpThreads * 2;  // kFastT == 2 in every form
     const int64_t blocks = (p.count + per - 1) / per;
-    switch (g_interp_fast_form.load()) {
-    case 1:
+    if (g_interp_fast_form.load() == 1)
         interp_image_fast_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
-        break;
-    case 2:
-        interp_image_pack_kernel<1><<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
-        break;
-    default:
-        interp_image_pack_kernel<0><<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
-    }
+    else
+        interp_image_pack_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
     return cudaGetLastError();
 }
 
 cudaError_t launch_interp_normals_fast(const InterpParams &p, cudaStream_t stream) {
     if (p.count <= 0) return cudaSuccess;
-    const int64_t blocks = (p.count + kInterpThreads - 1) / kInterpThreads;
-    interp_normals_fast_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+    if (g_interp_fast_form.load() == 1) {
+        const int64_t blocks = (p.count + kInterpThreads - 1) / kInterpThreads;
+        interp_normals_fast_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+    } else {
+        const int64_t per = (int64_t)kInterpThreads * 2;
+        const int64_t blocks = (p.count + per - 1) / per;
+        interp_normals_pack_kernel<<<(unsigned)blocks, kInterpThreads, 0, stream>>>(p);
+    }
     return cudaGetLastError();
 }
 

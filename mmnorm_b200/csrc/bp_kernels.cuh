@@ -92,6 +92,9 @@ struct BwdParams {
 // length of one antenna's staged grid row (N + W - 1 cells, so that no tap run wraps).
 constexpr int kNuW = 8;
 __host__ __device__ constexpr int nufft_row(int n) { return n + kNuW - 1; }
+// Row length of the forward's (G.re, G.im) rows: nufft_row rounded up to an even number of
+// 8-byte cells, so that every row, stage and bulk copy stays a multiple of 16 bytes.
+__host__ __device__ constexpr int nufft_row_fwd(int n) { return (nufft_row(n) + 1) & ~1; }
 
 cudaError_t launch_bwd_stage(const float *meas, int A, int F, int Fp, double k0, double kd,
                              int layout, void *dst, cudaStream_t stream);

@@ -157,7 +157,8 @@ __global__ void nufft_tables_kernel(int F, int N, int J0, double *__restrict__ s
 // rows[a][jj] = (G'_k.re, G_k.re, G'_k.im, G_k.im) for cell k = (jj - (W/2 - 1)) mod N,
 // jj < N + W - 1: a tap run starting at any cell reads W consecutive entries.  FWD_ONLY:
 // the forward reads only G, so its rows are (G_k.re, G_k.im) -- 8 bytes a cell -- and the
-// G' sums are not formed.
+// G' sums are not formed; those rows carry one more cell (never read) to an even length,
+// which keeps them multiples of 16 bytes for the bulk copies.
 template <bool FWD_ONLY>
 __global__ void nufft_grid_kernel(const float2 *__restrict__ meas, int F, int N, int J0, int row,
                                   double k0, double kd, const double *__restrict__ sc,
@@ -677,7 +678,7 @@ cudaError_t launch_nufft_grid(const float *meas, int A, int F, int N, int J0, do
                               double kd, const double *sc, const double2 *tw, void *rows,
                               bool fwd_only, cudaStream_t stream) {
     const int nt = 256;
-    const int row = nufft_row(N);
+    const int row = fwd_only ? nufft_row_fwd(N) : nufft_row(N);
     const int bpr = (row + nt - 1) / nt;
     const unsigned grid = (unsigned)((int64_t)A * bpr);
     const float2 *m = reinterpret_cast<const float2 *>(meas);

@@ -37,11 +37,21 @@ struct Stage {
         unsigned char *st = base + s * stage_bytes;
         const uint32_t ant_bytes = (uint32_t)(na * sizeof(AntRec));
         const uint32_t meas_bytes = (uint32_t)((size_t)na * fp * esz);
+        unsigned char *mdst = st + (size_t)nas * sizeof(AntRec);
+        const unsigned char *msrc =
+            static_cast<const unsigned char *>(p.meas) + (size_t)a0 * fp * esz;
+        // A bulk copy needs 16-byte aligned addresses and a size that is a multiple of 16
+        // bytes; a layout that breaks this is refused here (status word, barrier completed
+        // with no bytes) instead of faulting the copy engine.
+        if (((uintptr_t)st | (uintptr_t)mdst | (uintptr_t)msrc |
+             (uintptr_t)(p.ant + a0) | ant_bytes | meas_bytes) & 15u) {
+            set_status(p.status, MMN_ERR_INVALID_ARGUMENT);
+            mbar_arrive(&bars[s]);
+            return;
+        }
         mbar_arrive_expect_tx(&bars[s], ant_bytes + meas_bytes);
         bulk_g2s(st, p.ant + a0, ant_bytes, &bars[s]);
-        bulk_g2s(st + (size_t)nas * sizeof(AntRec),
-                 static_cast<const unsigned char *>(p.meas) + (size_t)a0 * fp * esz,
-                 meas_bytes, &bars[s]);
+        bulk_g2s(mdst, msrc, meas_bytes, &bars[s]);
     }
     __device__ void issue(const FwdParams &p, int c, int a_begin, int a_end) const {
         issue(p, c, c & 1, a_begin, a_end);

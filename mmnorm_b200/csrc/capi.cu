@@ -815,9 +815,10 @@ int plan_nufft_forward(const mmn_problem *p, NuFwdPlan *pl) {
     const int A = p->num_antennas, F = p->num_samples;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     pl->n = 2 * F;
-    pl->row = nufft_row(pl->n);
+    pl->row = nufft_row_fwd(pl->n);  // even: rows of 16-byte multiples
     const int rec = (int)sizeof(AntRec) + pl->row * 8;  // (G.re, G.im) cells
     if (rec > kMaxStageBytes) return MMN_ERR_TOO_LARGE;
+    if ((pl->row * 8) % 16 != 0) return MMN_ERR_UNSUPPORTED;  // bulk copies need 16 B rows
     pl->fn = fwd_nufft_kernel_ptr(&pl->threads, &pl->vpt);
     pl->ant_per_stage = std::max(1, std::min(16, 24 * 1024 / rec));
     pl->smem = 128 + 2 * (size_t)pl->ant_per_stage * rec;
@@ -949,7 +950,7 @@ extern "C" int mmn_backproject_nufft(const mmn_problem *p, float *image, float *
 }
 
 extern "C" int mmn_set_interp_fast_form(int32_t form) {
-    if (form < 0 || form > 2) return MMN_ERR_INVALID_ARGUMENT;
+    if (form < 0 || form > 1) return MMN_ERR_INVALID_ARGUMENT;
     g_interp_fast_form.store(form);
     return MMN_OK;
 }

@@ -239,13 +239,12 @@ def set_position_pass(form):
     _lib.check(_lib.load().mmn_set_position_pass(POSITION_PASSES[form]), "mmn_set_position_pass")
 
 
-INTERP_FAST_FORMS = {"packed": 0, "scalar": 1, "packed_alt_order": 2}
+INTERP_FAST_FORMS = {"packed": 0, "scalar": 1}
 
 
 def set_interp_fast_form(form):
-    """Form of the fast interpolated image pass: "packed" (default; two voxels per thread in
-    packed FP32 instructions), "scalar", or "packed_alt_order" (packed with the other FMA
-    order of the squared range)."""
+    """Form of the fast interpolated passes: "packed" (default; two voxels per thread in
+    packed FP32 instructions) or "scalar"."""
     _lib.check(_lib.load().mmn_set_interp_fast_form(INTERP_FAST_FORMS[form]),
                "mmn_set_interp_fast_form")
 

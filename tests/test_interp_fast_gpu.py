@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 TOL = 2e-6
 TOL_WORKLOAD = 1e-5
 
-FORMS = ["packed", "scalar", "packed_alt_order"]
+FORMS = ["packed", "scalar"]
 
 
 @pytest.fixture
@@ -121,8 +121,9 @@ def test_fast_image_vs_reference_kernel(cuda_dev, R, ti, fast_form):
     assert _rel(fast, ref) < TOL
 
 
+@pytest.mark.parametrize("fast_form", FORMS, indirect=True)
 @pytest.mark.parametrize("R", [1, 4])
-def test_fast_sn_est_vs_reference_kernel(cuda_dev, R):
+def test_fast_sn_est_vs_reference_kernel(cuda_dev, R, fast_form):
     import torch
     from mmnorm_b200 import _lib, ops
     from oracle import ref_cuda
@@ -266,7 +267,8 @@ def test_fast_at_the_full_workload(cuda_dev, fast_form):
     """128^3 voxels, 128x128 antennas, a 4096-bin range FFT of the 256-sample workload:
     fast image and vote within 1e-5 of the bit-exact kernel, for every form of the fast
     image pass (a squared range one ulp off the reference's moves the phase by ~1e-4 rad,
-    so a form whose FMA order differs from the reference's shows here)."""
+    so a form whose FMA contraction order differs from the reference's fails here: the
+    order fma(dz, dz, fma(dy, dy, dx*dx)) measured 2.5e-4)."""
     import torch
     from mmnorm_b200 import ops
     sc = scenes.config1(sign=-1, device=cuda_dev)
