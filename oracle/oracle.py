@@ -165,20 +165,24 @@ def full_backward(vox, ant, rx_offsets, meas, wavelength, slope, gI, gW, is_ti=F
 
 
 # ----------------------------------------------------------- numpy restatement (tiny)
-def full_np(vox, ant, rx_offsets, meas, wavelength, slope, is_ti=False):
-    """Pure-numpy FP64 full matched-filter image and vote; O(nv*na*ns) memory-light."""
-    vox = np.asarray(vox, dtype=np.float32).astype(np.float64)
-    ant = np.asarray(ant, dtype=np.float32).astype(np.float64)
-    rxo = np.asarray(rx_offsets, dtype=np.float32).reshape(-1, 3).astype(np.float64)
-    meas = np.asarray(meas).astype(np.complex64).astype(np.complex128)
+def full_np(vox, ant, rx_offsets, meas, wavelength, slope, is_ti=False, precision="f64"):
+    """Pure-numpy full matched-filter image and vote; O(nv*na*ns) memory-light.
+    precision "f64" (default): every step in FP64 on float32-rounded inputs; "f32": the
+    same formula with every array in float32 / complex64 (range, phase, exponential and
+    sums), the straightforward single-precision CPU version."""
+    fdt, cdt = (np.float64, np.complex128) if precision == "f64" else (np.float32, np.complex64)
+    vox = np.asarray(vox, dtype=np.float32).astype(fdt)
+    ant = np.asarray(ant, dtype=np.float32).astype(fdt)
+    rxo = np.asarray(rx_offsets, dtype=np.float32).reshape(-1, 3).astype(fdt)
+    meas = np.asarray(meas).astype(np.complex64).astype(cdt)
     na, ns = meas.shape
     o = rxo[np.arange(na) % rxo.shape[0]]
-    k = 2 * math.pi * (1.0 / wavelength + np.arange(ns) * slope / C)
+    k = (2 * math.pi * (1.0 / wavelength + np.arange(ns) * slope / C)).astype(fdt)
     diff = vox[:, None, :] - ant[None, :, :]                                # [nv, na, 3]
     d = np.linalg.norm(diff, axis=2) + np.linalg.norm(diff - o[None], axis=2)
     if is_ti:
-        d = d + 0.15
-    c = np.einsum("vaf,af->va", np.exp(-1j * d[:, :, None] * k[None, None, :]), meas)
+        d = d + fdt(0.15)
+    c = np.einsum("vaf,af->va", np.exp(cdt(-1j) * (d[:, :, None] * k[None, None, :])), meas)
     u = (ant + o / 2)[None, :, :] - vox[:, None, :]
     return c.sum(axis=1), np.einsum("va,vak->vk", c, u)
 

@@ -125,3 +125,17 @@ def test_normals_epilogue_restatement(oracle):
     raw1 = np.real(c * np.conj(I[0])) / abs(I[0]) * u
     _, _, r = oracle.normals_from_vote(I[:1], (c * u)[None, :], 0.0)
     np.testing.assert_allclose(r[0], raw1, rtol=1e-12)
+
+
+def test_numpy_restatement_in_fp32_tracks_fp64():
+    """The FP32 NumPy variant (bench's FP32 CPU baseline) computes the same formula in
+    single precision: complex64 outputs within the FP32 phase error of the FP64 form."""
+    from mmnorm_b200 import scenes
+    from oracle import oracle as O
+    sc = scenes.sphere_scene(seed=1, n_ap=6, nf=16, n_vox=3, n_pts=10)
+    args = (sc.voxel_centres(), sc.antenna_locs, np.zeros((1, 3)), sc.meas, sc.wavelength,
+            sc.slope)
+    I64, W64 = O.full_np(*args)
+    I32, W32 = O.full_np(*args, precision="f32")
+    assert I32.dtype == np.complex64 and I64.dtype == np.complex128
+    assert O.rel_l2(I32, I64) < 1e-3 and O.rel_l2(W32, W64) < 1e-3
