@@ -1,7 +1,9 @@
 """mmn_backproject_noalloc: the backprojection entry point for callers that cannot
-allocate device memory (stream capture, hosts that forbid allocation after start-up,
-real-time loops).  It must give the same image and vote as mmn_backproject, call after
-call, and refuse problems whose scratch would not fit its built-in 16 MiB array.
+allocate device memory where they image (hosts that own the whole device pool and forbid
+allocation after start-up, plugin hosts that pass only raw device pointers, real-time
+loops that must not block on the allocator).  It must give the same image and vote as
+mmn_backproject, call after call, report a clean status word after a normal call, and
+refuse problems whose scratch would not fit its built-in 16 MiB array.
 
 This file is collected last on purpose: the entry point's first call on a device
 performs its one-time set-up, and the test must pass both in a fresh process and after
