@@ -43,6 +43,9 @@ constexpr int kFormMixedPair = 0;    // FFMA2 voxel pairs, (re,re,im,im) samples
 constexpr int kFormMixedScalar = 1;  // scalar FFMA, (re,im) samples
 constexpr int kFormPlain = 2;        // FP32 sincosf per sample, (re,im) samples
 constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im_a') samples
+// voxel pairs as kFormMixedPair, each 32-sample block evaluated as two independent 16-step
+// Horner chains joined by one multiply with z^16 (two dependency chains per thread)
+constexpr int kFormMixedPairSplit = 4;
 
 // Block anchors: kAnchorPoly recomputes exp(-j d kappa_{32b}) per block from the FP64
 // phase (FP64 quarter-turn reduction + FP32 Taylor polynomials); kAnchorFixed steps a
@@ -67,12 +70,14 @@ constexpr int kAnchorFixed2 = 2;
 template <int T, int NT, int FORM, int ANCHOR, bool PERSISTENT>
 __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                                         unsigned char *smem, uint32_t &gchunk) {
-    static_assert(FORM != kFormMixedPair || T % 2 == 0, "pair form needs an even T");
+    static_assert((FORM != kFormMixedPair && FORM != kFormMixedPairSplit) || T % 2 == 0,
+                  "pair form needs an even T");
+    constexpr bool kPairRows = FORM == kFormMixedPair || FORM == kFormMixedPairSplit;
     Stage st;
     st.bars = reinterpret_cast<uint64_t *>(smem);
     st.base = smem + 128;
     st.nas = p.ant_per_stage;
-    st.esz = FORM == kFormMixedPair ? 16 : 8;  // antenna pairs: 16 B per pair = 8 B per antenna
+    st.esz = kPairRows ? 16 : 8;  // antenna pairs: 16 B per pair = 8 B per antenna
     st.fp = p.fp;
     st.stage_bytes = (size_t)st.nas * sizeof(AntRec) + (size_t)st.nas * st.fp * st.esz;
     float *kappa_tab = reinterpret_cast<float *>(st.base + 2 * st.stage_bytes);  // PLAIN only
@@ -224,8 +229,9 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
         for (int a = 0; a < na; ++a) {
             const AntRec &ar = ants[a];
             float cr[T], ci[T];
-            if constexpr (FORM == kFormMixedPair) {
+            if constexpr (kPairRows) {
                 constexpr int P = T / 2;
+                constexpr bool kSplit = FORM == kFormMixedPairSplit;
                 const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * fp;
                 double d[T];
                 unsigned long long ph[T], stp[T];
@@ -263,25 +269,79 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                         c2r[q] = c2i[q] = make_float2(0.f, 0.f);
                     }
                 }
+                // z^16 by four complex squarings (split form only)
+                float2 z16r[P], z16i[P], nz16i[P];
+                if constexpr (kSplit) {
+#pragma unroll
+                    for (int q = 0; q < P; ++q) {
+                        float2 ar2 = zr[q], ai2 = zi[q];
+#pragma unroll
+                        for (int k2 = 0; k2 < 4; ++k2) {
+                            const float2 nr = __ffma2_rn(ar2, ar2, __fmul2_rn(ai2, make_float2(-ai2.x, -ai2.y)));
+                            ai2 = __fmul2_rn(__fadd2_rn(ar2, ar2), ai2);
+                            ar2 = nr;
+                        }
+                        z16r[q] = ar2;
+                        z16i[q] = ai2;
+                        nz16i[q] = make_float2(-ai2.x, -ai2.y);
+                    }
+                }
                 for (int b = 0; b < nblk; ++b) {
                     const float4 *mb = m4 + b * kBlockF;
                     float2 hr[P], hi[P];
-                    const float4 top = mb[kBlockF - 1];
-#pragma unroll
-                    for (int q = 0; q < P; ++q) {
-                        hr[q] = make_float2(top.x, top.y);
-                        hi[q] = make_float2(top.z, top.w);
-                    }
-#pragma unroll
-                    for (int t = kBlockF - 2; t >= 0; --t) {
-                        const float4 mm = mb[t];
-                        const float2 mr = make_float2(mm.x, mm.y), mi = make_float2(mm.z, mm.w);
+                    if constexpr (kSplit) {
+                        constexpr int H = kBlockF / 2;
+                        float2 hrb[P], hib[P];
+                        const float4 topa = mb[H - 1], topb = mb[kBlockF - 1];
 #pragma unroll
                         for (int q = 0; q < P; ++q) {
-                            const float2 u = __ffma2_rn(hr[q], zr[q], mr);
-                            const float2 w = __ffma2_rn(hr[q], zi[q], mi);
-                            hr[q] = __ffma2_rn(hi[q], nzi[q], u);
-                            hi[q] = __ffma2_rn(hi[q], zr[q], w);
+                            hr[q] = make_float2(topa.x, topa.y);
+                            hi[q] = make_float2(topa.z, topa.w);
+                            hrb[q] = make_float2(topb.x, topb.y);
+                            hib[q] = make_float2(topb.z, topb.w);
+                        }
+#pragma unroll
+                        for (int t = H - 2; t >= 0; --t) {
+                            const float4 ma = mb[t], mbb = mb[H + t];
+                            const float2 mra = make_float2(ma.x, ma.y), mia = make_float2(ma.z, ma.w);
+                            const float2 mrb = make_float2(mbb.x, mbb.y), mib = make_float2(mbb.z, mbb.w);
+#pragma unroll
+                            for (int q = 0; q < P; ++q) {
+                                const float2 ua = __ffma2_rn(hr[q], zr[q], mra);
+                                const float2 wa = __ffma2_rn(hr[q], zi[q], mia);
+                                const float2 ub = __ffma2_rn(hrb[q], zr[q], mrb);
+                                const float2 wb = __ffma2_rn(hrb[q], zi[q], mib);
+                                hr[q] = __ffma2_rn(hi[q], nzi[q], ua);
+                                hi[q] = __ffma2_rn(hi[q], zr[q], wa);
+                                hrb[q] = __ffma2_rn(hib[q], nzi[q], ub);
+                                hib[q] = __ffma2_rn(hib[q], zr[q], wb);
+                            }
+                        }
+                        // h = h_low + z^16 h_high
+#pragma unroll
+                        for (int q = 0; q < P; ++q) {
+                            const float2 r2 = __ffma2_rn(z16r[q], hrb[q], __ffma2_rn(nz16i[q], hib[q], hr[q]));
+                            hi[q] = __ffma2_rn(z16r[q], hib[q], __ffma2_rn(z16i[q], hrb[q], hi[q]));
+                            hr[q] = r2;
+                        }
+                    } else {
+                        const float4 top = mb[kBlockF - 1];
+#pragma unroll
+                        for (int q = 0; q < P; ++q) {
+                            hr[q] = make_float2(top.x, top.y);
+                            hi[q] = make_float2(top.z, top.w);
+                        }
+#pragma unroll
+                        for (int t = kBlockF - 2; t >= 0; --t) {
+                            const float4 mm = mb[t];
+                            const float2 mr = make_float2(mm.x, mm.y), mi = make_float2(mm.z, mm.w);
+#pragma unroll
+                            for (int q = 0; q < P; ++q) {
+                                const float2 u = __ffma2_rn(hr[q], zr[q], mr);
+                                const float2 w = __ffma2_rn(hr[q], zi[q], mi);
+                                hr[q] = __ffma2_rn(hi[q], nzi[q], u);
+                                hi[q] = __ffma2_rn(hi[q], zr[q], w);
+                            }
                         }
                     }
 #pragma unroll
@@ -580,6 +640,10 @@ const FwdVariant *fwd_variants(int *count) {
     // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
         {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed>()},
+        // each block as two 16-step chains joined by z^16 (kFormMixedPairSplit)
+        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPairSplit, kAnchorFixed2>(), "mixed_split_fx2_t2_n128_s24", 1, pers_ptr<2, 128, kFormMixedPairSplit, kAnchorFixed2>(), 24 * 1024},
+        {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPairSplit, kAnchorFixed2>(), "mixed_split_fx2_t2_n256", 1, pers_ptr<2, 256, kFormMixedPairSplit, kAnchorFixed2>()},
+        {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPairSplit, kAnchorFixed2>(), "mixed_split_fx2_t2_n128_s16", 1, pers_ptr<2, 128, kFormMixedPairSplit, kAnchorFixed2>(), 16 * 1024},
         // the cheaper prologue (kAnchorFixed2)
         {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n128_s24", 1, pers_ptr<2, 128, kFormMixedPair, kAnchorFixed2>(), 24 * 1024},
         {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed2>(), "mixed_ffma2_fx2_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed2>()},
