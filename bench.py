@@ -32,7 +32,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "G voxel*antenna*frequency updates/s (fused image + normal vote, mixed FP64/FP32)"
+METRIC = "G voxel·ant·freq updates/s, mixed vs plain FP32 on 1 B200 at ≤1e-4 L2 err"  # fused image + normal vote
 UNIT = "G updates/s"
 
 
