@@ -64,7 +64,10 @@ def image_and_normals(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offse
     ``radar_data``: (A, S, R) complex raw samples (the FFT is applied here in
     interpolated mode); ``antenna_locs``: (A, 3) TX positions; ``rx_offsets``: (R, 3).
     ``num_samples`` is the chirp's sample count (the range-bin spacing uses it,
-    py_image_gpu.py:270).  Returns device tensors:
+    py_image_gpu.py:270).  ``precision``: the full matched filter's form ("mixed", "plain",
+    "nufft"); in interpolated mode "fast" selects the fast form (the reference's range
+    bins, hardware sine/cosine phasor) and anything else the reference's arithmetic.
+    Returns device tensors:
 
       sum_image    complex64 [NX, NY, NZ], normalised as image_cuda does
       normals      float32 [NX, NY, NZ, 3] unit vectors, NaN outside the mask
@@ -93,7 +96,9 @@ def image_and_normals(x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_offse
             a0, a1 = g * MAX_NUM_ANT // R, min(A, (g + 1) * MAX_NUM_ANT // R)
             rows = virtual_rows(data[a0:a1])
             locs = ant64[a0:a1].to(f32).repeat_interleave(R, dim=0).contiguous()
-            img_g, vote_g = ops.backproject(x, y, z, locs, rxo, rows, wl, sl, mode="interp",
+            img_g, vote_g = ops.backproject(x, y, z, locs, rxo, rows, wl, sl,
+                                            mode="interp_fast" if precision == "fast"
+                                            else "interp",
                                             fft_spacing=spacing, is_ti_radar=is_ti_radar)
             img_g /= (a1 - a0)
             image = img_g if image is None else image.add_(img_g)

@@ -138,3 +138,22 @@ def test_normal_data_file_matches_loader_format(cuda_dev, tmp_path):
     np.testing.assert_array_equal(l_n, nrm)
     np.testing.assert_array_equal(l_ant, cl)
     np.testing.assert_array_equal(l_ch, meas)
+
+
+def test_interpolated_mode_fast_form(cuda_dev, oracle):
+    """precision="fast" in the stage-1 driver: the fast form of interpolated mode against
+    the reference-exact kernels on the same device FFT (same bins; the phasor differs by
+    ~5e-7 per term)."""
+    from mmnorm_b200 import stage1
+    sc, data, rxo, bw = _case(seed=5, R=2, n_ap=6, nf=64)
+    args = (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs.astype(np.float64), data, rxo,
+            sc.slope, sc.wavelength, bw, data.shape[1])
+    img_e, _, nrm_e, _, _ = stage1.generate_mmwave_surface_normals(
+        *args, is_ti_radar=True, use_interpolated_processing=True)
+    img_f, _, nrm_f, _, _ = stage1.generate_mmwave_surface_normals(
+        *args, is_ti_radar=True, use_interpolated_processing=True, precision="fast")
+    assert oracle.rel_l2(img_f, img_e) <= 2e-6
+    m = ~np.isnan(nrm_e[..., 0])
+    assert m.sum() > 0
+    np.testing.assert_array_equal(~np.isnan(nrm_f[..., 0]), m)
+    assert np.median(_angle(nrm_f[m], nrm_e[m])) < 1e-4
