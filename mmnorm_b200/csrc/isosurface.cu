@@ -183,15 +183,15 @@ __device__ float value_at(const IsoParams &p, const float *g, float tau, float p
         g100 < kUndef + 10 || g110 < kUndef + 10 || g101 < kUndef + 10 || g111 < kUndef + 10)
         return kMinStep;
     const float tx = (px - (p.bb_min_x + mx * voxel_size)) / voxel_size;
-    const float c01 = (1.f - tx) * g000 + tx * g100;
-    const float c23 = (1.f - tx) * g010 + tx * g110;
-    const float c45 = (1.f - tx) * g001 + tx * g101;
-    const float c67 = (1.f - tx) * g011 + tx * g111;
+    const float ex_y0z0 = (1.f - tx) * g000 + tx * g100;
+    const float ex_y1z0 = (1.f - tx) * g010 + tx * g110;
+    const float ex_y0z1 = (1.f - tx) * g001 + tx * g101;
+    const float ex_y1z1 = (1.f - tx) * g011 + tx * g111;
     const float ty = (py - (p.bb_min_y + my * voxel_size)) / voxel_size;
-    const float c0 = (1.f - ty) * c01 + ty * c23;
-    const float c1 = (1.f - ty) * c45 + ty * c67;
+    const float fz0 = (1.f - ty) * ex_y0z0 + ty * ex_y1z0;
+    const float fz1 = (1.f - ty) * ex_y0z1 + ty * ex_y1z1;
     const float tz = (pz - (p.bb_min_z + mz * voxel_size)) / voxel_size;
-    return (1.f - tz) * c0 + tz * c1;
+    return (1.f - tz) * fz0 + tz * fz1;
 }
 
 // marches one ray; on a hit returns true with the rough point and its voxel index
@@ -247,15 +247,15 @@ __device__ bool refine(const IsoParams &p, const float *g, float tau, float hx, 
         return __fadd_rn(__fmul_rn(__fsub_rn(1.f, t), a), __fmul_rn(t, b));
     };
     const float tx = __fdiv_rn(__fsub_rn(hx, mnx), vs);
-    const float c01 = lerp(tx, at(x, y, z), at(x + 1, y, z));
-    const float c23 = lerp(tx, at(x, y + 1, z), at(x + 1, y + 1, z));
-    const float c45 = lerp(tx, at(x, y, z + 1), at(x + 1, y, z + 1));
-    const float c67 = lerp(tx, at(x, y + 1, z + 1), at(x + 1, y + 1, z + 1));
+    const float ex_y0z0 = lerp(tx, at(x, y, z), at(x + 1, y, z));
+    const float ex_y1z0 = lerp(tx, at(x, y + 1, z), at(x + 1, y + 1, z));
+    const float ex_y0z1 = lerp(tx, at(x, y, z + 1), at(x + 1, y, z + 1));
+    const float ex_y1z1 = lerp(tx, at(x, y + 1, z + 1), at(x + 1, y + 1, z + 1));
     const float ty = __fdiv_rn(__fsub_rn(hy, mny), vs);
-    const float c0 = lerp(ty, c01, c23);
-    const float c1 = lerp(ty, c45, c67);
+    const float fz0 = lerp(ty, ex_y0z0, ex_y1z0);
+    const float fz1 = lerp(ty, ex_y0z1, ex_y1z1);
     const float tz = __fdiv_rn(__fsub_rn(hz, mnz), vs);
-    const float sdf = lerp(tz, c0, c1);
+    const float sdf = lerp(tz, fz0, fz1);
     ix = __fadd_rn(hx, __fmul_rn(dx, sdf));
     iy = __fadd_rn(hy, __fmul_rn(dy, sdf));
     iz = __fadd_rn(hz, __fmul_rn(dz, sdf));
