@@ -84,6 +84,36 @@ def test_interpolation_form_and_probe_validation_without_device():
         _lib.MMN_ERR_INVALID_ARGUMENT
 
 
+def test_interpolated_fast_form_validation_without_device():
+    """The fast interpolated form's selector and entry points check their arguments before
+    any device call: bad form, bad mode, missing fft_spacing, too many bins, null output."""
+    from mmnorm_b200 import _lib
+    h = _lib.load()
+    assert h.mmn_set_interp_fast_form(2) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_set_interp_fast_form(-1) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_set_interp_fast_form(1) == _lib.MMN_OK
+    assert h.mmn_set_interp_fast_form(0) == _lib.MMN_OK  # the default, set again
+    p = _lib.MmnProblem()
+    p.num_x = p.num_y = p.num_z = 4
+    p.num_rx = 1
+    p.num_samples = 4096
+    p.wavelength = 3.9e-3
+    dummy = ctypes.c_void_p(256)
+    p.x_locs = p.y_locs = p.z_locs = dummy
+    # interpolated modes need a positive fft_spacing
+    assert h.mmn_workspace_bytes(ctypes.byref(p), _lib.MODE_INTERP_FAST, 1) == 0
+    p.fft_spacing = 2.3e-3
+    assert h.mmn_workspace_bytes(ctypes.byref(p), _lib.MODE_INTERP_FAST, 1) == 256
+    p.num_samples = (1 << 22) + 1  # beyond the fast form's rounding-constant bins
+    assert h.mmn_workspace_bytes(ctypes.byref(p), _lib.MODE_INTERP_FAST, 1) == 0
+    assert h.mmn_backproject(ctypes.byref(p), _lib.MODE_INTERP_FAST, None, None, None, 0,
+                             None) == _lib.MMN_ERR_TOO_LARGE
+    assert h.mmn_backproject(ctypes.byref(p), 4, None, None, None, 0, None) == \
+        _lib.MMN_ERR_INVALID_ARGUMENT
+    args = [None] * 15 + [0.0, 3.9e-3, 2.3e-3, 4, 4, 4, 16, 1, 8, 64, 0, 0, -1, None, 0, None]
+    assert h.mmn_cuda_sn_est_fast(*args) == _lib.MMN_ERR_NULL_POINTER
+
+
 def test_library_is_sm100a_only_build():
     """The build recipe targets exactly sm_100a."""
     from mmnorm_b200 import build
