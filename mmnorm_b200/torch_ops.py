@@ -19,7 +19,7 @@ from torch import Tensor
 
 from . import ops
 
-_MODES = ("mixed", "plain", "interp", "nufft")
+_MODES = ("mixed", "plain", "interp", "interp_fast", "nufft")
 
 
 @torch.library.custom_op("mmnorm::backproject", mutates_args=())

@@ -290,3 +290,16 @@ def test_fast_at_the_full_workload(cuda_dev, fast_form):
     print("fast (%s) vs bit-exact at the workload: image %.2e vote %.2e"
           % (fast_form, e_img, e_vote))
     assert e_img < TOL_WORKLOAD and e_vote < TOL_WORKLOAD
+
+
+def test_fast_form_through_torch_operator(cuda_dev):
+    import torch
+    import mmnorm_b200.torch_ops  # noqa: F401
+    d = _setup(cuda_dev, R=2)
+    i0, v0 = _backproject(d, "interp_fast")
+    i1, v1 = torch.ops.mmnorm.backproject(d["x"], d["y"], d["z"], d["ant"], d["rxo"], d["fft"],
+                                          float(d["wl"]), float(d["slope"]), "interp_fast",
+                                          float(d["fsp"]), bool(d["ti"]), None)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(i1.cpu().numpy().ravel(), i0)
+    np.testing.assert_array_equal(v1.cpu().numpy().reshape(3, -1), v0)
