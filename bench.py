@@ -354,8 +354,9 @@ def ours_arm(args):
         img_a, vote_a, _, _ = step()
         acc_mixed = subset(img_a, vote_a)
         del img_a, vote_a
-    # prep_antennas, stage_meas, bp_fwd_kernel (+ bp_reduce_partials), max_abs, normals
-    launches_per_step = 5 + (1 if plan["splits"] > 1 else 0)
+    # the library's count for backproject (prep_antennas, stage_meas when the form needs a
+    # staged copy, bp_fwd_kernel, bp_reduce_partials when split) + max_abs + normals
+    launches_per_step = plan["launches"] + 2
 
     out = {}
     if rank == 0 and world == 1 and args.plain_steps > 0:
@@ -573,8 +574,7 @@ def ours_arm(args):
             "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
-            "precision": "mixed: FP64 range and phase wrap, FP32 Horner rotation recurrence "
-                         "re-anchored every 32 samples, FP32 accumulation",
+            "precision": precision_text(variant["name"]),
             "data": "synthetic (seeded point-scatterer scene, exp(-j4pi f r/c)/r^2, 15 dB)",
             "config": {"workload": sc.name + " (128^3 voxels @2 mm, 128x128 antennas @2 mm, "
                        "256 freqs 77-81 GHz; image + vote + unit normals)",
@@ -699,6 +699,7 @@ def time_batched(dev, replays=3):
                  antenna_locs=t(sc.antenna_locs), rx_offsets=t(np.zeros((1, 3), np.float32)),
                  meas=t(sc.meas), wavelength=sc.wavelength, slope=sc.slope) for sc in scs]
     updates = sum(sc.updates for sc in scs)
+    single_variant = ops.current_variant("mixed")
     tuned = autotune.tune_batched(objs)
     plan = ops.BatchPlan(objs, items_per_slot=tuned["best"])
     plan.capture()
@@ -725,11 +726,13 @@ def time_batched(dev, replays=3):
         for a, b in ((img, si), (vote, sv)):
             worst = max(worst, float((a - b).abs().norm() / b.abs().norm()))
     info = plan.info()
+    ops.set_variant("mixed", single_variant)  # the other legs keep the workload's pick
     return {"objects": len(objs), "updates": updates, "ms": ms,
             "value": updates / (ms * 1e-3) / 1e9, "unit": UNIT,
             "one_by_one_ms": ms_single, "one_by_one_value": updates / (ms_single * 1e-3) / 1e9,
             "max_rel_l2_vs_one_by_one": worst, "items": info["items"], "ctas": info["ctas"],
-            "items_per_slot": tuned["best"], "autotune_ms": tuned["times_ms"],
+            "items_per_slot": tuned["best"], "variant": tuned["variant"],
+            "autotune_ms": tuned["times_ms"],
             "graph": "captured once, replayed"}
 
 
@@ -1154,7 +1157,21 @@ def accuracy_report(dev, sc, idx, sub_mixed, sub_plain, max_mixed, max_plain):
 # one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum on one full-size launch
 # (a one-pass metric set, checked on the small case first), summarised in
 # profiles/bp_fwd_kernel_dram_boxcyl128.md.  Variants without a capture report null.
-FWD_DRAM_BYTES_PER_LAUNCH = {"mixed_antpair_fx2_t1_n256": 38597632 + 37433856}
+FWD_DRAM_BYTES_PER_LAUNCH = {"mixed_antpair_fx2_t1_n256": 38597632 + 37433856,
+                             "mixed_clen64_fx2_t4_n128_s24": 40073728 + 36137728}
+
+
+def precision_text(variant_name):
+    """The arithmetic of a mixed-form kernel variant, for the bench line."""
+    if "clen" in variant_name:
+        blk = 64 if "clen64" in variant_name else 32
+        rec = ("FP32 second-order (Clenshaw) rotation recurrence b_t = m_t + 2cos(theta) "
+               "b_{t+1} - b_{t+2}, first-order Horner where |cos theta| > 0.98")
+    else:
+        blk = 32
+        rec = "FP32 first-order Horner rotation recurrence"
+    return ("mixed: FP64 range and phase wrap; %s; re-anchored every %d samples; FP32 "
+            "accumulation" % (rec, blk))
 
 
 def main():

@@ -87,16 +87,22 @@ size_t mmn_workspace_bytes(const mmn_problem *p, int32_t mode, int32_t want_vote
 /* Kernel variants of the full-mode forward pass (voxels per thread x threads per CTA)
  * for the autotuner; no reference counterpart (the reference has one fixed launch,
  * block=512, py_image_gpu.py:272-273).  mmn_set_variant selects the process-wide
- * variant mmn_backproject uses for MMN_MODE_MIXED / MMN_MODE_PLAIN. */
+ * variant mmn_backproject uses for MMN_MODE_MIXED / MMN_MODE_PLAIN; mmn_get_variant
+ * returns the selected index (or MMN_ERR_INVALID_ARGUMENT for another mode). */
 int mmn_num_variants(int32_t mode);
 int mmn_variant_info(int32_t mode, int32_t idx, int32_t *voxels_per_thread, int32_t *threads);
 int mmn_set_variant(int32_t mode, int32_t idx);
+int mmn_get_variant(int32_t mode);
 const char *mmn_variant_name(int32_t mode, int32_t idx); /* NULL for a bad index */
 
 /* The decomposition mmn_backproject will use for `p`: voxel tiles, antenna splits,
  * antennas per shared-memory stage, threads per CTA, voxels per thread. */
 int mmn_plan_info(const mmn_problem *p, int32_t mode, int32_t *tiles, int32_t *splits,
                   int32_t *ant_per_stage, int32_t *threads, int32_t *voxels_per_thread);
+/* Kernel launches mmn_backproject makes for `p` in `mode` (full modes): antenna records,
+ * the staging copy of the sample rows when the kernel form needs one, the forward kernel,
+ * and the split reduction when the antenna range is split.  No reference counterpart. */
+int mmn_plan_launches(const mmn_problem *p, int32_t mode, int32_t *launches);
 
 /*
  * Fused backprojection + vote.  image: complex64 [V] raw sum over all virtual

@@ -90,8 +90,10 @@ SIGNATURES = [
     ("mmn_num_variants", _I, [_I32]),
     ("mmn_variant_info", _I, [_I32, _I32, _I32P, _I32P]),
     ("mmn_set_variant", _I, [_I32, _I32]),
+    ("mmn_get_variant", _I, [_I32]),
     ("mmn_variant_name", ctypes.c_char_p, [_I32, _I32]),
     ("mmn_plan_info", _I, [_PROB, _I32, _I32P, _I32P, _I32P, _I32P, _I32P]),
+    ("mmn_plan_launches", _I, [_PROB, _I32, _I32P]),
     ("mmn_backproject", _I, [_PROB, _I32, _P, _P, _P, _SZ, _P]),
     ("mmn_backproject_noalloc", _I, [_PROB, _I32, _P, _P, _P]),
     ("mmn_noalloc_read_status", _I, [_I32P, _P]),

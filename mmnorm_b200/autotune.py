@@ -84,27 +84,44 @@ def tune(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slo
     return res
 
 
-def tune_batched(objects, options=(4, 8, 16), repeats=1):
-    """Times the batched persistent launch for each work granularity (items per resident
-    CTA) and returns {"best": items_per_slot, "times_ms": {...}}."""
+def tune_batched(objects, options=(4, 8, 16), variants=None, repeats=1, apply=True):
+    """Times the batched persistent launch for each (mixed kernel variant, work granularity
+    in items per resident CTA) and returns {"best": items_per_slot, "variant": name,
+    "times_ms": {"name|items": ms}}.  ``variants``: names to try (default: the current
+    variant and the fastest of each block length among the second-order and Horner forms
+    that the single-object autotuner would consider); the objects' sample counts differ, and
+    a variant with 64-sample blocks pads every row to a multiple of 64.  With ``apply`` the
+    winning variant is made current (a BatchPlan takes the current variant when built)."""
+    names = [v["name"] for v in ops.variants("mixed")]
+    cur = ops.current_variant("mixed")
+    if variants is None:
+        variants = [names[cur]]
+        for cand in ("mixed_clen64_fx2_t4_n128_s24", "mixed_clen_fx2_t4_n128_s24",
+                     "mixed_antpair_fx2_t1_n256"):
+            if cand in names and cand not in variants:
+                variants.append(cand)
     times = {}
-    for ips in options:
-        plan = ops.BatchPlan(objects, items_per_slot=ips)
-        plan.run()
-        torch.cuda.synchronize()
-        best = float("inf")
-        for _ in range(repeats):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
+    for name in variants:
+        ops.set_variant("mixed", names.index(name))
+        for ips in options:
+            plan = ops.BatchPlan(objects, items_per_slot=ips)
             plan.run()
-            e1.record()
             torch.cuda.synchronize()
-            best = min(best, e0.elapsed_time(e1))
-        times[ips] = best
-        del plan
-    best_ips = min(times, key=times.get)
-    return {"best": best_ips, "times_ms": {str(k): v for k, v in times.items()}}
+            best = float("inf")
+            for _ in range(repeats):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                plan.run()
+                e1.record()
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            times[(name, ips)] = best
+            del plan
+    best_name, best_ips = min(times, key=times.get)
+    ops.set_variant("mixed", names.index(best_name) if apply else cur)
+    return {"best": best_ips, "variant": best_name,
+            "times_ms": {"%s|%d" % k: v for k, v in times.items()}}
 
 
 def tune_position(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope,

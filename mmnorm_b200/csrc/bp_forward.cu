@@ -23,6 +23,10 @@
 // slot): each Horner step of a voxel pair is 4 FFMA2, reading the sample from a
 // (re, re, im, im) record so one broadcast 16-byte shared load feeds both halves.
 // The scalar-FFMA version of the same kernel is kept as an autotuner variant.
+// The second-order variants (mixed_clen*) take the same block sums from Clenshaw's
+// recurrence b_t = m_t + 2 cos(theta) b_{t+1} - b_{t+2}, whose multiplier is real: one
+// FADD2 + FFMA2 per sample and (voxel, antenna), complex b packed as (re, im), plain
+// (re, im) samples, and no operand duplication -- the FP32 pipe runs closer to its peak.
 //
 // PLAIN form.  FP32 distance and FP32 phase -d*kappa_j with one sincosf per sample,
 // then a complex multiply-add -- the straightforward FP32 kernel.
@@ -46,6 +50,13 @@ constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im
 // voxel pairs as kFormMixedPair, each 32-sample block evaluated as two independent 16-step
 // Horner chains joined by one multiply with z^16 (two dependency chains per thread)
 constexpr int kFormMixedPairSplit = 4;
+// second-order (Clenshaw) form of the block sum, (re, im) samples: see fwd_item
+constexpr int kFormMixedClen = 5;
+constexpr int kFormMixedClen64 = 6;  // the same with 64-sample blocks (rows padded to 64)
+// The second-order form is used for a warp's (voxels, antenna) pairs when every lane's
+// per-sample rotation z = e^{-i theta} has |cos theta| <= kClenMaxCos (theta in
+// [0.2, pi - 0.2]); otherwise that antenna's blocks run the first-order Horner form.
+constexpr float kClenMaxCos = 0.98f;
 
 // Block anchors: kAnchorPoly recomputes exp(-j d kappa_{32b}) per block from the FP64
 // phase (FP64 quarter-turn reduction + FP32 Taylor polynomials); kAnchorFixed steps a
@@ -369,6 +380,132 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                     ci[2 * q] = c2i[q].x;
                     ci[2 * q + 1] = c2i[q].y;
                 }
+            } else if constexpr (FORM == kFormMixedClen || FORM == kFormMixedClen64) {
+                // Second-order form.  With z = e^{i phi}, z^{t+1} = 2 cos(phi) z^t - z^{t-1},
+                // so the block sum h = sum_{t<L} m_t z^t follows from the backward recurrence
+                //     b_t = m_t + c2 b_{t+1} - b_{t+2},  c2 = 2 cos(phi),  b_L = b_{L+1} = 0,
+                //     h = b_0 - conj(z) b_1
+                // (Clenshaw's summation for a three-term recurrence).  The multiplier is real,
+                // so each (voxel, antenna) chain keeps its complex b as one (re, im) register
+                // pair: one FADD2 + one FFMA2 per sample (4 lane operations, as the Horner step),
+                // and one 16-byte shared load feeds two samples to every voxel of the thread.
+                // Blocks are L = 32 or 64 samples long (kFormMixedClen64: half the re-anchoring).
+                // Error: a rounding error made at step t reaches b_0 scaled by at most
+                // min(t + 1, 1 / |sin phi|), and for rows dominated by a few scatterers (input
+                // near the recurrence's own modes e^{+-i phi t}) |b| grows to ~L|m| / sin phi,
+                // so each block sum carries several times the Horner form's error (measured on
+                // the 128^3 workload: 6.9e-6 (L = 32) and 8.8e-6 (L = 64) image relative L2
+                // against FP64, Horner 2.6e-6).  The form is kept away from phi near 0 and pi
+                // (kClenMaxCos); there the same blocks run the first-order Horner form.
+                static_assert(T % 2 == 0, "the second-order form takes voxels in pairs");
+                constexpr int L = FORM == kFormMixedClen64 ? 64 : kBlockF;
+                constexpr int LSH = FORM == kFormMixedClen64 ? 6 : 5;
+                const int nblk_c = fp / L;
+                const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
+                unsigned long long ph[T], stp[T];
+                float zr[T], zi[T];
+                float2 c2[T];
+                bool clen = true;
+                {
+                    int32_t za[T];
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        const double d = range_fp64_newton((double)vx[k], (double)vy[k],
+                                                           (double)vz[k], ar, mono, p.ti);
+                        const unsigned long long u = turns_fixed64(-d * p.tsmp);
+                        za[k] = (int32_t)(u >> 32);
+                        stp[k] = u << LSH;
+                        ph[k] = turns_fixed_top(-d * p.t0);
+                        cr[k] = ci[k] = 0.f;
+                    }
+#pragma unroll
+                    for (int q = 0; q < T / 2; ++q) {
+                        float2 c, s, ns;
+                        cis_turns_pair(za[2 * q], za[2 * q + 1], c, s, ns);
+                        zr[2 * q] = c.x;
+                        zr[2 * q + 1] = c.y;
+                        zi[2 * q] = s.x;
+                        zi[2 * q + 1] = s.y;
+                    }
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        c2[k] = make_float2(2.f * zr[k], 2.f * zr[k]);
+                        clen = clen && fabsf(zr[k]) <= kClenMaxCos;
+                    }
+                }
+                clen = __all_sync(0xffffffffu, clen);
+                for (int b = 0; b < nblk_c; ++b) {
+                    const float4 *mb = m4 + b * (L / 2);
+                    float sr[T], si[T];
+                    const float4 top = mb[L / 2 - 1];  // samples L-2, L-1
+                    if (clen) {
+                        float2 b1[T], b2[T];
+#pragma unroll
+                        for (int k = 0; k < T; ++k) {
+                            b2[k] = make_float2(top.z, top.w);  // b_{L-1} = m_{L-1}
+                            b1[k] = __ffma2_rn(c2[k], b2[k], make_float2(top.x, top.y));  // b_{L-2}
+                        }
+#pragma unroll
+                        for (int q = L / 2 - 2; q >= 0; --q) {
+                            const float4 mm = mb[q];
+#pragma unroll
+                            for (int k = 0; k < T; ++k) {
+                                const float2 dd = __fadd2_rn(make_float2(mm.z, mm.w),
+                                                             make_float2(-b2[k].x, -b2[k].y));
+                                b2[k] = b1[k];
+                                b1[k] = __ffma2_rn(c2[k], b1[k], dd);
+                            }
+#pragma unroll
+                            for (int k = 0; k < T; ++k) {
+                                const float2 dd = __fadd2_rn(make_float2(mm.x, mm.y),
+                                                             make_float2(-b2[k].x, -b2[k].y));
+                                b2[k] = b1[k];
+                                b1[k] = __ffma2_rn(c2[k], b1[k], dd);
+                            }
+                        }
+                        // h = b_0 - conj(z) b_1   (b1 = b_0, b2 = b_1)
+#pragma unroll
+                        for (int k = 0; k < T; ++k) {
+                            sr[k] = fmaf(-zr[k], b2[k].x, fmaf(-zi[k], b2[k].y, b1[k].x));
+                            si[k] = fmaf(-zr[k], b2[k].y, fmaf(zi[k], b2[k].x, b1[k].y));
+                        }
+                    } else {
+                        // first-order Horner, h <- h z + m_t
+#pragma unroll
+                        for (int k = 0; k < T; ++k) {
+                            sr[k] = top.z;
+                            si[k] = top.w;
+                            const float u = fmaf(sr[k], zr[k], top.x);
+                            const float w = fmaf(sr[k], zi[k], top.y);
+                            sr[k] = fmaf(-si[k], zi[k], u);
+                            si[k] = fmaf(si[k], zr[k], w);
+                        }
+#pragma unroll 1
+                        for (int q = L / 2 - 2; q >= 0; --q) {
+                            const float4 mm = mb[q];
+#pragma unroll
+                            for (int k = 0; k < T; ++k) {
+                                float u = fmaf(sr[k], zr[k], mm.z);
+                                float w = fmaf(sr[k], zi[k], mm.w);
+                                sr[k] = fmaf(-si[k], zi[k], u);
+                                si[k] = fmaf(si[k], zr[k], w);
+                                u = fmaf(sr[k], zr[k], mm.x);
+                                w = fmaf(sr[k], zi[k], mm.y);
+                                sr[k] = fmaf(-si[k], zi[k], u);
+                                si[k] = fmaf(si[k], zr[k], w);
+                            }
+                        }
+                    }
+                    // re-anchor with the exact block phase
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        float anr, ani;
+                        fixed_cis(ph[k], anr, ani);
+                        ph[k] += stp[k];
+                        cr[k] = fmaf(anr, sr[k], fmaf(-ani, si[k], cr[k]));
+                        ci[k] = fmaf(anr, si[k], fmaf(ani, sr[k], ci[k]));
+                    }
+                }
             } else if constexpr (FORM == kFormMixedScalar) {
                 const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
                 double d[T];
@@ -674,6 +811,15 @@ const FwdVariant *fwd_variants(int *count) {
         // two voxel pairs per thread: one shared load feeds 8 FFMA2 (the stages limit
         // occupancy to two CTAs per SM either way, which leaves 128 registers a thread)
         {4, 256, false, 16, fwd_ptr<4, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t4_n256", 1, pers_ptr<4, 256, kFormMixedPair, kAnchorFixed>()},
+        // second-order (Clenshaw) block sums over (re, im) samples, one FADD2 + FFMA2 per
+        // sample and chain
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen, kAnchorFixed2>()},
+        {2, 128, false, 8, fwd_ptr<2, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t2_n128_s24", 0, pers_ptr<2, 128, kFormMixedClen, kAnchorFixed2>(), 24 * 1024},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen, kAnchorFixed2>()},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), 24 * 1024},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 24 * 1024, 64},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 0, 64},
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), 0, 64},
         {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256", 0, nullptr},
         {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128", 0, nullptr},
         {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128", 0, nullptr},

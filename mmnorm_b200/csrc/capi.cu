@@ -75,7 +75,7 @@ int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int 
     const bool pairs = pl->var->layout == 2;
     pl->a_pad = pairs ? A + (A & 1) : A;
     A = pl->a_pad;
-    pl->fp = (F + kBlockF - 1) / kBlockF * kBlockF;
+    pl->fp = fwd_row_samples(*pl->var, F);
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
     const int esz = pl->var->esz;
     const int rec = (int)sizeof(AntRec) + pl->fp * esz;
@@ -267,6 +267,20 @@ int mmn_set_variant(int32_t mode, int32_t idx) {
     return MMN_ERR_INVALID_ARGUMENT;
 }
 
+int mmn_get_variant(int32_t mode) {
+    if (mode != MMN_MODE_MIXED && mode != MMN_MODE_PLAIN) return MMN_ERR_INVALID_ARGUMENT;
+    int n = 0;
+    const FwdVariant *v = fwd_variants(&n);
+    const int cur = g_variant[mode == MMN_MODE_PLAIN ? 1 : 0].load();
+    int c = 0;
+    for (int i = 0; i < n; ++i) {
+        if (v[i].plain != (mode == MMN_MODE_PLAIN)) continue;
+        if (i == cur) return c;
+        ++c;
+    }
+    return 0;  // the stored index is not of this mode's list: mmn_backproject uses the first
+}
+
 const char *mmn_variant_name(int32_t mode, int32_t idx) {
     int n = 0;
     const FwdVariant *v = fwd_variants(&n);
@@ -306,6 +320,22 @@ int mmn_plan_info(const mmn_problem *p, int32_t mode, int32_t *tiles, int32_t *s
     if (ant_per_stage) *ant_per_stage = pl.ant_per_stage;
     if (threads) *threads = pl.var->nt;
     if (voxels_per_thread) *voxels_per_thread = pl.var->t;
+    return MMN_OK;
+}
+
+int mmn_plan_launches(const mmn_problem *p, int32_t mode, int32_t *launches) {
+    if (!launches) return MMN_ERR_NULL_POINTER;
+    int rc = check_problem(p, mode);
+    if (rc != MMN_OK) return rc;
+    if (is_interp(mode)) return MMN_ERR_INVALID_ARGUMENT;
+    const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
+    FwdPlan pl;
+    rc = plan_forward(nvox, 0, nvox, p->num_antennas, p->num_samples, mode, aligned16(p->meas),
+                      false, &pl);
+    if (rc != MMN_OK) return rc;
+    // antenna records, the staging copy (a layout other than the caller's rows, padding,
+    // or misaligned rows), the forward kernel, the split reduction
+    *launches = 1 + (pl.copy_meas ? 1 : 0) + 1 + (pl.splits > 1 ? 1 : 0);
     return MMN_OK;
 }
 
@@ -1287,7 +1317,7 @@ extern "C" int mmn_batch_create(const mmn_problem *problems, int32_t num_objects
     for (int o = 0; o < num_objects; ++o) {
         auto &ob = b->obj[o];
         const mmn_problem &p = problems[o];
-        ob.fp = (p.num_samples + kBlockF - 1) / kBlockF * kBlockF;
+        ob.fp = fwd_row_samples(*b->var, p.num_samples);
         if (ob.fp > kMaxFp) {
             delete b;
             return MMN_ERR_TOO_LARGE;

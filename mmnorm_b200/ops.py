@@ -98,7 +98,12 @@ def plan_info(problem, mode="mixed"):
                                    *[ctypes.byref(v) for v in vals])
     _lib.check(rc, "mmn_plan_info")
     keys = ("tiles", "splits", "antennas_per_stage", "threads", "voxels_per_thread")
-    return {k: v.value for k, v in zip(keys, vals)}
+    out = {k: v.value for k, v in zip(keys, vals)}
+    n = ctypes.c_int32()
+    _lib.check(_lib.load().mmn_plan_launches(ctypes.byref(problem), _lib.MODES[mode],
+                                             ctypes.byref(n)), "mmn_plan_launches")
+    out["launches"] = n.value  # kernels backproject launches for this problem
+    return out
 
 
 def backproject(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slope, *,
@@ -227,6 +232,11 @@ def variants(mode="mixed"):
 
 def set_variant(mode, index):
     _lib.check(_lib.load().mmn_set_variant(_lib.MODES[mode], int(index)), "mmn_set_variant")
+
+
+def current_variant(mode="mixed"):
+    """Index (into ``variants(mode)``) of the process-wide variant ``backproject`` uses."""
+    return int(_lib.load().mmn_get_variant(_lib.MODES[mode]))
 
 
 POSITION_PASSES = {"interp": 0, "horner": 1}

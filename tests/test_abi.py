@@ -51,6 +51,13 @@ def test_version_and_validation_without_device():
     # the no-alloc status accessor checks its output pointer before touching a device
     assert h.mmn_noalloc_read_status(None, None) == _lib.MMN_ERR_NULL_POINTER
     assert h.mmn_set_variant(7, 0) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_get_variant(7) == _lib.MMN_ERR_INVALID_ARGUMENT
+    assert h.mmn_plan_launches(ctypes.byref(p), 0, None) == _lib.MMN_ERR_NULL_POINTER
+    n = h.mmn_num_variants(_lib.MODE_MIXED)
+    assert h.mmn_set_variant(_lib.MODE_MIXED, n - 1) == _lib.MMN_OK
+    assert h.mmn_get_variant(_lib.MODE_MIXED) == n - 1
+    assert h.mmn_set_variant(_lib.MODE_MIXED, 0) == _lib.MMN_OK
+    assert h.mmn_get_variant(_lib.MODE_MIXED) == 0
     assert h.mmn_num_variants(_lib.MODE_MIXED) >= 1
     assert h.mmn_num_variants(_lib.MODE_PLAIN) >= 1
 
