@@ -12,21 +12,20 @@
 // sum_i Re(c_i conj(I))/|I| * u_i; that equals Re(conj(I) * W)/|I|, so one pass
 // with 8 FP32 accumulators per voxel gives the image and the un-normalised normal.
 //
-// MIXED form (default).  Per (voxel, antenna): d in FP64; the sample sum is split
-// into blocks of 32 samples, each evaluated by Horner's rule in FP32,
-//     h_b = sum_{t<32} m[i, 32b+t] * z^t,   z = exp(-j d kappa_step)   (4 FMA / sample)
-// i.e. the rotation recurrence is applied to the running partial sum instead of to a
-// separate phasor, and every block is re-anchored with the exact FP64-wrapped phase
-//     c_i += exp(-j d kappa_{32b}) * h_b.
-// The per-sample work is one complex multiply-add, no SFU.  The default kernel runs a
-// thread's voxels in PAIRS with Blackwell's packed FFMA2 (two FP32 FMAs per issue
-// slot): each Horner step of a voxel pair is 4 FFMA2, reading the sample from a
-// (re, re, im, im) record so one broadcast 16-byte shared load feeds both halves.
-// The scalar-FFMA version of the same kernel is kept as an autotuner variant.
-// The second-order variants (mixed_clen*) take the same block sums from Clenshaw's
-// recurrence b_t = m_t + 2 cos(theta) b_{t+1} - b_{t+2}, whose multiplier is real: one
-// FADD2 + FFMA2 per sample and (voxel, antenna), complex b packed as (re, im), plain
-// (re, im) samples, and no operand duplication -- the FP32 pipe runs closer to its peak.
+// MIXED form.  Per (voxel, antenna): d in FP64; the sample sum is split into blocks of
+// L = 32 (or 64) samples, each summed in FP32 by a rotation recurrence with
+// z = exp(-j d kappa_step), and every block is re-anchored with the exact FP64-wrapped
+// phase
+//     c_i += exp(-j d kappa_{L b}) * h_b,   h_b = sum_{t<L} m[i, L b + t] * z^t.
+// The per-sample work is 4 FP32 lane operations, no SFU, in one of two recurrences:
+//  * second-order (Clenshaw) -- the default variant and the autotuner's usual pick:
+//    b_t = m_t + 2 cos(theta) b_{t+1} - b_{t+2}, h_b = b_0 - conj(z) b_1.  The multiplier
+//    is real, so a (voxel, antenna) chain is one (re, im) register pair: one FADD2 + one
+//    FFMA2 (Blackwell's packed FP32) per sample on plain (re, im) samples, one 16-byte
+//    shared load feeding two samples to each of the thread's voxels;
+//  * first-order Horner, h <- h z + m_t (one complex multiply-add): voxel pairs or
+//    antenna pairs in the halves of FFMA2 (the sample duplicated into (re, re, im, im)
+//    or antenna-pair records), or scalar FFMA.
 //
 // PLAIN form.  FP32 distance and FP32 phase -d*kappa_j with one sincosf per sample,
 // then a complex multiply-add -- the straightforward FP32 kernel.
@@ -776,6 +775,8 @@ static const void *pers_ptr() {
 const FwdVariant *fwd_variants(int *count) {
     // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
+        // default: second-order block sums, 32-sample blocks, 4 voxels per thread
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), 24 * 1024},
         {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed>()},
         // each block as two 16-step chains joined by z^16 (kFormMixedPairSplit)
         {2, 128, false, 16, fwd_ptr<2, 128, kFormMixedPairSplit, kAnchorFixed2>(), "mixed_split_fx2_t2_n128_s24", 1, pers_ptr<2, 128, kFormMixedPairSplit, kAnchorFixed2>(), 24 * 1024},
@@ -816,7 +817,6 @@ const FwdVariant *fwd_variants(int *count) {
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen, kAnchorFixed2>()},
         {2, 128, false, 8, fwd_ptr<2, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t2_n128_s24", 0, pers_ptr<2, 128, kFormMixedClen, kAnchorFixed2>(), 24 * 1024},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen, kAnchorFixed2>()},
-        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), 24 * 1024},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 24 * 1024, 64},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 0, 64},
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), 0, 64},

@@ -89,7 +89,9 @@ def test_noalloc_interpolated_mode(cuda_dev):
 def test_noalloc_rejects_problems_beyond_its_scratch(cuda_dev):
     from mmnorm_b200 import _lib
     sc = scenes.sphere_scene(seed=32, n_ap=4, nf=16, n_vox=4, n_pts=5)
-    A, F = 8192, 256  # staged samples alone need 32 MiB > 16 MiB
+    # 250 samples are not a whole number of blocks, so every kernel form stages padded
+    # rows: at least 16384 x 256 x 8 bytes = 32 MiB > 16 MiB
+    A, F = 16384, 250
     meas = np.zeros((A, F), np.complex64)
     ant = np.zeros((A, 3), np.float32)
     ant[:, 2] = -0.1
@@ -113,16 +115,18 @@ def test_noalloc_status_word_reads_ok_after_a_call(cuda_dev):
 
 
 def test_noalloc_just_under_its_scratch_limit(cuda_dev):
-    """4000 antennas x 256 samples: 256 + 64*4000 + 16*4000*256 bytes of records and
-    staged samples: 16,640,256 of the array's 16,777,216 bytes."""
+    """The default kernel form stages (re, im) rows padded to 32 samples when the sample
+    count is not a multiple of 32: 7940 antennas x 250 samples take 256 + 64*7940 +
+    8*7940*256 = 16,769,536 of the array's 16,777,216 bytes."""
     import torch
     from mmnorm_b200 import _lib, ops
-    sc = scenes.sphere_scene(seed=34, n_ap=4, nf=256, n_vox=8, n_pts=20)
-    A, F = 4000, 256
+    ops.set_variant("mixed", 0)  # the default form, whose scratch the sizes above assume
+    sc = scenes.sphere_scene(seed=34, n_ap=4, nf=250, n_vox=8, n_pts=20)
+    A, F = 7940, 250
     rng = np.random.default_rng(34)
     meas = (rng.standard_normal((A, F)) + 1j * rng.standard_normal((A, F))).astype(np.complex64)
     g = np.arange(A)
-    ant = np.stack([(g % 80 - 40) * 2e-3, (g // 80 - 25) * 2e-3, np.zeros(A)], 1)
+    ant = np.stack([(g % 80 - 40) * 2e-3, (g // 80 - 50) * 2e-3, np.zeros(A)], 1)
     args = _tensors(cuda_dev, sc, meas=meas, ant=ant.astype(np.float32))
     ref_img, ref_vote = ops.backproject(*args, sc.wavelength, sc.slope, mode="mixed")
     for _ in range(2):
