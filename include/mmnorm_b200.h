@@ -204,10 +204,11 @@ void mmn_batch_destroy(mmn_batch *batch);
  * as mmn_backproject; the scratch comes from a 16 MiB device array built into the
  * library, which every GPU (every CUDA context) that loads the library holds until the
  * process exits.
- *   - Limit: the antenna records plus the staged samples must fit 16 MiB (about
- *     256 + 64*A + 16*A*roundup(F, 32) bytes in the default form, e.g. A*F up to about
- *     one million antenna-samples); larger problems return MMN_ERR_TOO_LARGE before
- *     anything runs.  Every voxel tile takes the whole antenna range (no antenna split),
+ *   - Limit: the antenna records plus the staged samples must fit 16 MiB: 256 + 64*A
+ *     bytes, plus 8*A*roundup(F, 32) when the default form stages the rows (F not a
+ *     multiple of 32, or rows not 16-byte aligned; 16 bytes per sample in the first-order
+ *     voxel-pair variants), e.g. A*F up to about two million antenna-samples when staged;
+ *     larger problems return MMN_ERR_TOO_LARGE before anything runs.  Every voxel tile takes the whole antenna range (no antenna split),
  *     so problems with few voxels run slower than through mmn_backproject.
  *   - The array's device address belongs to a CUDA context.  The first call in each
  *     context (normally the device's primary context) looks it up with
