@@ -89,8 +89,8 @@ def tune_batched(objects, options=(4, 8, 16), variants=None, repeats=1, apply=Tr
     in items per resident CTA) and returns {"best": items_per_slot, "variant": name,
     "times_ms": {"name|items": ms}}.  ``variants``: names to try (default: the current
     variant and the fastest of each block length among the second-order and Horner forms
-    that the single-object autotuner would consider); the objects' sample counts differ, and
-    a variant with 64-sample blocks pads every row to a multiple of 64.  With ``apply`` the
+    that the single-object autotuner would consider), since the objects' sample counts and
+    grids differ from the single-object problems the variants were tuned on.  With ``apply`` the
     winning variant is made current (a BatchPlan takes the current variant when built)."""
     names = [v["name"] for v in ops.variants("mixed")]
     cur = ops.current_variant("mixed")

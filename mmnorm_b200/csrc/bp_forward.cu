@@ -51,7 +51,7 @@ constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im
 constexpr int kFormMixedPairSplit = 4;
 // second-order (Clenshaw) form of the block sum, (re, im) samples: see fwd_item
 constexpr int kFormMixedClen = 5;
-constexpr int kFormMixedClen64 = 6;  // the same with 64-sample blocks (rows padded to 64)
+constexpr int kFormMixedClen64 = 6;  // the same with 64-sample blocks (+ a last 32 if needed)
 // The second-order form is used for a warp's (voxels, antenna) pairs when every lane's
 // per-sample rotation z = e^{-i theta} has |cos theta| <= kClenMaxCos (theta in
 // [0.2, pi - 0.2]); otherwise that antenna's blocks run the first-order Horner form.
@@ -69,6 +69,74 @@ constexpr int kAnchorFixed = 1;
 // conversion), the rotation z from u's top word (integer quarter turns + FP32 Taylor),
 // the block step as u << 5 and the start phase rounded to 2^-33 turns.
 constexpr int kAnchorFixed2 = 2;
+
+// One block of the second-order form (see fwd_item): the sums h_k = sum_{t<L} m_t z_k^t of
+// the thread's T voxels against one antenna, from L samples (re, im) at mb (two per
+// 16-byte load), by Clenshaw's recurrence when `clen`, else by first-order Horner.
+template <int T, int L>
+__device__ __forceinline__ void clen_block(const float4 *mb, bool clen, const float2 (&c2)[T],
+                                           const float (&zr)[T], const float (&zi)[T],
+                                           float (&sr)[T], float (&si)[T]) {
+    const float4 top = mb[L / 2 - 1];  // samples L-2, L-1
+    if (clen) {
+        float2 b1[T], b2[T];
+#pragma unroll
+        for (int k = 0; k < T; ++k) {
+            b2[k] = make_float2(top.z, top.w);  // b_{L-1} = m_{L-1}
+            b1[k] = __ffma2_rn(c2[k], b2[k], make_float2(top.x, top.y));  // b_{L-2}
+        }
+#pragma unroll
+        for (int q = L / 2 - 2; q >= 0; --q) {
+            const float4 mm = mb[q];
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const float2 dd = __fadd2_rn(make_float2(mm.z, mm.w),
+                                             make_float2(-b2[k].x, -b2[k].y));
+                b2[k] = b1[k];
+                b1[k] = __ffma2_rn(c2[k], b1[k], dd);
+            }
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const float2 dd = __fadd2_rn(make_float2(mm.x, mm.y),
+                                             make_float2(-b2[k].x, -b2[k].y));
+                b2[k] = b1[k];
+                b1[k] = __ffma2_rn(c2[k], b1[k], dd);
+            }
+        }
+        // h = b_0 - conj(z) b_1   (b1 = b_0, b2 = b_1)
+#pragma unroll
+        for (int k = 0; k < T; ++k) {
+            sr[k] = fmaf(-zr[k], b2[k].x, fmaf(-zi[k], b2[k].y, b1[k].x));
+            si[k] = fmaf(-zr[k], b2[k].y, fmaf(zi[k], b2[k].x, b1[k].y));
+        }
+    } else {
+        // first-order Horner, h <- h z + m_t
+#pragma unroll
+        for (int k = 0; k < T; ++k) {
+            sr[k] = top.z;
+            si[k] = top.w;
+            const float u = fmaf(sr[k], zr[k], top.x);
+            const float w = fmaf(sr[k], zi[k], top.y);
+            sr[k] = fmaf(-si[k], zi[k], u);
+            si[k] = fmaf(si[k], zr[k], w);
+        }
+#pragma unroll 1
+        for (int q = L / 2 - 2; q >= 0; --q) {
+            const float4 mm = mb[q];
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                float u = fmaf(sr[k], zr[k], mm.z);
+                float w = fmaf(sr[k], zi[k], mm.w);
+                sr[k] = fmaf(-si[k], zi[k], u);
+                si[k] = fmaf(si[k], zr[k], w);
+                u = fmaf(sr[k], zr[k], mm.x);
+                w = fmaf(sr[k], zi[k], mm.y);
+                sr[k] = fmaf(-si[k], zi[k], u);
+                si[k] = fmaf(si[k], zr[k], w);
+            }
+        }
+    }
+}
 
 // One work item: voxel tile `tile` of p against antenna split `split`.  The two stage
 // buffers' mbarriers are initialised by the caller; `gchunk` counts the chunks this CTA
@@ -388,7 +456,8 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                 // so each (voxel, antenna) chain keeps its complex b as one (re, im) register
                 // pair: one FADD2 + one FFMA2 per sample (4 lane operations, as the Horner step),
                 // and one 16-byte shared load feeds two samples to every voxel of the thread.
-                // Blocks are L = 32 or 64 samples long (kFormMixedClen64: half the re-anchoring).
+                // Blocks are L = 32 or 64 samples long (kFormMixedClen64: half the re-anchoring;
+                // rows are padded to 32 samples, a last half block runs with L = 32).
                 // Error: a rounding error made at step t reaches b_0 scaled by at most
                 // min(t + 1, 1 / |sin phi|), and for rows dominated by a few scatterers (input
                 // near the recurrence's own modes e^{+-i phi t}) |b| grows to ~L|m| / sin phi,
@@ -434,67 +503,8 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                 }
                 clen = __all_sync(0xffffffffu, clen);
                 for (int b = 0; b < nblk_c; ++b) {
-                    const float4 *mb = m4 + b * (L / 2);
                     float sr[T], si[T];
-                    const float4 top = mb[L / 2 - 1];  // samples L-2, L-1
-                    if (clen) {
-                        float2 b1[T], b2[T];
-#pragma unroll
-                        for (int k = 0; k < T; ++k) {
-                            b2[k] = make_float2(top.z, top.w);  // b_{L-1} = m_{L-1}
-                            b1[k] = __ffma2_rn(c2[k], b2[k], make_float2(top.x, top.y));  // b_{L-2}
-                        }
-#pragma unroll
-                        for (int q = L / 2 - 2; q >= 0; --q) {
-                            const float4 mm = mb[q];
-#pragma unroll
-                            for (int k = 0; k < T; ++k) {
-                                const float2 dd = __fadd2_rn(make_float2(mm.z, mm.w),
-                                                             make_float2(-b2[k].x, -b2[k].y));
-                                b2[k] = b1[k];
-                                b1[k] = __ffma2_rn(c2[k], b1[k], dd);
-                            }
-#pragma unroll
-                            for (int k = 0; k < T; ++k) {
-                                const float2 dd = __fadd2_rn(make_float2(mm.x, mm.y),
-                                                             make_float2(-b2[k].x, -b2[k].y));
-                                b2[k] = b1[k];
-                                b1[k] = __ffma2_rn(c2[k], b1[k], dd);
-                            }
-                        }
-                        // h = b_0 - conj(z) b_1   (b1 = b_0, b2 = b_1)
-#pragma unroll
-                        for (int k = 0; k < T; ++k) {
-                            sr[k] = fmaf(-zr[k], b2[k].x, fmaf(-zi[k], b2[k].y, b1[k].x));
-                            si[k] = fmaf(-zr[k], b2[k].y, fmaf(zi[k], b2[k].x, b1[k].y));
-                        }
-                    } else {
-                        // first-order Horner, h <- h z + m_t
-#pragma unroll
-                        for (int k = 0; k < T; ++k) {
-                            sr[k] = top.z;
-                            si[k] = top.w;
-                            const float u = fmaf(sr[k], zr[k], top.x);
-                            const float w = fmaf(sr[k], zi[k], top.y);
-                            sr[k] = fmaf(-si[k], zi[k], u);
-                            si[k] = fmaf(si[k], zr[k], w);
-                        }
-#pragma unroll 1
-                        for (int q = L / 2 - 2; q >= 0; --q) {
-                            const float4 mm = mb[q];
-#pragma unroll
-                            for (int k = 0; k < T; ++k) {
-                                float u = fmaf(sr[k], zr[k], mm.z);
-                                float w = fmaf(sr[k], zi[k], mm.w);
-                                sr[k] = fmaf(-si[k], zi[k], u);
-                                si[k] = fmaf(si[k], zr[k], w);
-                                u = fmaf(sr[k], zr[k], mm.x);
-                                w = fmaf(sr[k], zi[k], mm.y);
-                                sr[k] = fmaf(-si[k], zi[k], u);
-                                si[k] = fmaf(si[k], zr[k], w);
-                            }
-                        }
-                    }
+                    clen_block<T, L>(m4 + b * (L / 2), clen, c2, zr, zi, sr, si);
                     // re-anchor with the exact block phase
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
@@ -503,6 +513,20 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                         ph[k] += stp[k];
                         cr[k] = fmaf(anr, sr[k], fmaf(-ani, si[k], cr[k]));
                         ci[k] = fmaf(anr, si[k], fmaf(ani, sr[k], ci[k]));
+                    }
+                }
+                if constexpr (L != kBlockF) {
+                    // rows are padded to 32 samples: a remaining half block of 32
+                    if (fp - nblk_c * L != 0) {
+                        float sr[T], si[T];
+                        clen_block<T, kBlockF>(m4 + nblk_c * (L / 2), clen, c2, zr, zi, sr, si);
+#pragma unroll
+                        for (int k = 0; k < T; ++k) {
+                            float anr, ani;
+                            fixed_cis(ph[k], anr, ani);
+                            cr[k] = fmaf(anr, sr[k], fmaf(-ani, si[k], cr[k]));
+                            ci[k] = fmaf(anr, si[k], fmaf(ani, sr[k], ci[k]));
+                        }
                     }
                 }
             } else if constexpr (FORM == kFormMixedScalar) {
@@ -817,9 +841,9 @@ const FwdVariant *fwd_variants(int *count) {
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen, kAnchorFixed2>()},
         {2, 128, false, 8, fwd_ptr<2, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t2_n128_s24", 0, pers_ptr<2, 128, kFormMixedClen, kAnchorFixed2>(), 24 * 1024},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen, kAnchorFixed2>()},
-        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 24 * 1024, 64},
-        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 0, 64},
-        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), 0, 64},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 24 * 1024},
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>()},
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>()},
         {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256", 0, nullptr},
         {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128", 0, nullptr},
         {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128", 0, nullptr},

@@ -46,14 +46,7 @@ struct FwdVariant {
     int layout; // staged sample layout (stage_meas): 0 (re,im), 1 (re,re,im,im), 2 antenna pairs
     const void *persistent_fn;  // bp_fwd_persistent instantiation of the same form, or null
     int max_stage_bytes;        // cap on one shared-memory stage; 0: the library default
-    int fblk;                   // samples per re-anchored block (rows padded to it); 0: 32
 };
-
-// Padded row length of a forward variant: F rounded up to the variant's anchor block.
-inline int fwd_row_samples(const FwdVariant &v, int F) {
-    const int b = v.fblk > 0 ? v.fblk : kBlockF;
-    return (F + b - 1) / b * b;
-}
 
 // Batched (persistent) forward: per-object FwdParams and a cost-sorted work list.
 struct BatchParams {

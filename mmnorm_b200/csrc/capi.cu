@@ -75,7 +75,7 @@ int plan_forward(int64_t nvox, int64_t vox_start, int64_t vox_count, int A, int 
     const bool pairs = pl->var->layout == 2;
     pl->a_pad = pairs ? A + (A & 1) : A;
     A = pl->a_pad;
-    pl->fp = fwd_row_samples(*pl->var, F);
+    pl->fp = (F + kBlockF - 1) / kBlockF * kBlockF;
     if (pl->fp > kMaxFp) return MMN_ERR_TOO_LARGE;
     const int esz = pl->var->esz;
     const int rec = (int)sizeof(AntRec) + pl->fp * esz;
@@ -1317,7 +1317,7 @@ extern "C" int mmn_batch_create(const mmn_problem *problems, int32_t num_objects
     for (int o = 0; o < num_objects; ++o) {
         auto &ob = b->obj[o];
         const mmn_problem &p = problems[o];
-        ob.fp = fwd_row_samples(*b->var, p.num_samples);
+        ob.fp = (p.num_samples + kBlockF - 1) / kBlockF * kBlockF;
         if (ob.fp > kMaxFp) {
             delete b;
             return MMN_ERR_TOO_LARGE;
