@@ -138,6 +138,50 @@ __device__ __forceinline__ void clen_block(const float4 *mb, bool clen, const fl
     }
 }
 
+// The last rem (< L) valid samples of a row, as clen_block with a runtime length: the
+// recurrence starts at b_rem = b_{rem+1} = 0, which is where the padded zeros above them
+// would have left it.
+template <int T>
+__device__ __forceinline__ void clen_partial(const float2 *m2, int rem, bool clen,
+                                             const float2 (&c2)[T], const float (&zr)[T],
+                                             const float (&zi)[T], float (&sr)[T],
+                                             float (&si)[T]) {
+    if (clen) {
+        float2 b1[T], b2[T];
+#pragma unroll
+        for (int k = 0; k < T; ++k) b1[k] = b2[k] = make_float2(0.f, 0.f);
+#pragma unroll 2
+        for (int t = rem - 1; t >= 0; --t) {
+            const float2 m = m2[t];
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const float2 dd = __fadd2_rn(m, make_float2(-b2[k].x, -b2[k].y));
+                b2[k] = b1[k];
+                b1[k] = __ffma2_rn(c2[k], b1[k], dd);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < T; ++k) {
+            sr[k] = fmaf(-zr[k], b2[k].x, fmaf(-zi[k], b2[k].y, b1[k].x));
+            si[k] = fmaf(-zr[k], b2[k].y, fmaf(zi[k], b2[k].x, b1[k].y));
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < T; ++k) sr[k] = si[k] = 0.f;
+#pragma unroll 1
+        for (int t = rem - 1; t >= 0; --t) {
+            const float2 m = m2[t];
+#pragma unroll
+            for (int k = 0; k < T; ++k) {
+                const float u = fmaf(sr[k], zr[k], m.x);
+                const float w = fmaf(sr[k], zi[k], m.y);
+                sr[k] = fmaf(-si[k], zi[k], u);
+                si[k] = fmaf(si[k], zr[k], w);
+            }
+        }
+    }
+}
+
 // One work item: voxel tile `tile` of p against antenna split `split`.  The two stage
 // buffers' mbarriers are initialised by the caller; `gchunk` counts the chunks this CTA
 // has consumed so far (stage = gchunk & 1, phase parity = (gchunk >> 1) & 1), so a
@@ -468,7 +512,8 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                 static_assert(T % 2 == 0, "the second-order form takes voxels in pairs");
                 constexpr int L = FORM == kFormMixedClen64 ? 64 : kBlockF;
                 constexpr int LSH = FORM == kFormMixedClen64 ? 6 : 5;
-                const int nblk_c = fp / L;
+                const int ns = p.nsmp > 0 ? p.nsmp : fp;  // valid samples per row
+                const int nblk_c = ns / L;
                 const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
                 unsigned long long ph[T], stp[T];
                 float zr[T], zi[T];
@@ -482,7 +527,7 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                                                            (double)vz[k], ar, mono, p.ti);
                         const unsigned long long u = turns_fixed64(-d * p.tsmp);
                         za[k] = (int32_t)(u >> 32);
-                        stp[k] = u << LSH;
+                        stp[k] = u << 5;  // 32 samples; an L-block steps stp << (LSH - 5)
                         ph[k] = turns_fixed_top(-d * p.t0);
                         cr[k] = ci[k] = 0.f;
                     }
@@ -502,32 +547,31 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                     }
                 }
                 clen = __all_sync(0xffffffffu, clen);
-                for (int b = 0; b < nblk_c; ++b) {
-                    float sr[T], si[T];
-                    clen_block<T, L>(m4 + b * (L / 2), clen, c2, zr, zi, sr, si);
-                    // re-anchor with the exact block phase
+                // whole L-sample blocks, then one block of the row's rem < L remaining valid
+                // samples, whose padded zeros are skipped (they add exactly nothing: the
+                // recurrence from the top of a zero run stays at zero)
+                auto anchor = [&](const float (&sr)[T], const float (&si)[T], int shift) {
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
                         float anr, ani;
                         fixed_cis(ph[k], anr, ani);
-                        ph[k] += stp[k];
+                        ph[k] += stp[k] << shift;
                         cr[k] = fmaf(anr, sr[k], fmaf(-ani, si[k], cr[k]));
                         ci[k] = fmaf(anr, si[k], fmaf(ani, sr[k], ci[k]));
                     }
+                };
+                for (int b = 0; b < nblk_c; ++b) {
+                    float sr[T], si[T];
+                    clen_block<T, L>(m4 + b * (L / 2), clen, c2, zr, zi, sr, si);
+                    anchor(sr, si, LSH - 5);
                 }
-                if constexpr (L != kBlockF) {
-                    // rows are padded to 32 samples: a remaining half block of 32
-                    if (fp - nblk_c * L != 0) {
-                        float sr[T], si[T];
-                        clen_block<T, kBlockF>(m4 + nblk_c * (L / 2), clen, c2, zr, zi, sr, si);
-#pragma unroll
-                        for (int k = 0; k < T; ++k) {
-                            float anr, ani;
-                            fixed_cis(ph[k], anr, ani);
-                            cr[k] = fmaf(anr, sr[k], fmaf(-ani, si[k], cr[k]));
-                            ci[k] = fmaf(anr, si[k], fmaf(ani, sr[k], ci[k]));
-                        }
-                    }
+                const int rem = ns - nblk_c * L;
+                const float4 *mr4 = m4 + nblk_c * (L / 2);
+                if (rem > 0) {
+                    float sr[T], si[T];
+                    clen_partial<T>(reinterpret_cast<const float2 *>(mr4), rem, clen, c2, zr, zi,
+                                    sr, si);
+                    anchor(sr, si, 0);
                 }
             } else if constexpr (FORM == kFormMixedScalar) {
                 const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);

@@ -19,7 +19,8 @@ struct FwdParams {
     int32_t num_ant;
     int32_t fp;
     int32_t ant_per_stage; // antennas per shared-memory stage
-    int32_t pad1;
+    int32_t nsmp;          // samples per row before padding (F); 0: fp (the second-order
+                           // forms skip the padded zeros of a row's last block)
     const int32_t *mono_flag; // device word: 1 when all RX offsets are zero
     double k0, kd;         // 2*pi/lambda, 2*pi*slope/c
     double t0, tblk;       // 1/lambda and 32*slope/c: turns per metre of range

@@ -172,6 +172,7 @@ int run_forward(const FwdPlan &pl, const mmn_problem *p, const float *meas_r,
     fp.meas = meas;
     fp.num_ant = pl.a_pad;
     fp.fp = pl.fp;
+    fp.nsmp = F;
     fp.ant_per_stage = pl.ant_per_stage;
     fp.mono_flag = hdr + 1;
     fp.k0 = 2.0 * kPi / p->wavelength;
@@ -1429,6 +1430,7 @@ extern "C" int mmn_batch_upload(mmn_batch *b, void *workspace, size_t workspace_
         f.meas = ws + ob.off_meas;
         f.num_ant = ob.a_pad;
         f.fp = ob.fp;
+        f.nsmp = p.num_samples;
         f.ant_per_stage = ob.nas;
         f.mono_flag = reinterpret_cast<const int32_t *>(ws + b->off_flags) + o;
         f.k0 = 2.0 * kPi / p.wavelength;

@@ -83,8 +83,8 @@ def test_small_angle_runs_the_first_order_form(cuda_dev, oracle):
 
 @pytest.mark.parametrize("nf", [2, 63, 64, 65, 130])
 def test_second_order_range_and_padding(cuda_dev, oracle, nf):
-    """Sample counts around the 32- and 64-sample blocks (rows zero-padded to 32 samples; a
-    64-sample form ends a row of an odd number of 32-sample blocks with one block of 32)."""
+    """Sample counts around the 32- and 64-sample blocks: whole blocks, then a last block
+    over the row's remaining valid samples (the zeros padding rows to 32 are skipped)."""
     sc = scenes.sphere_scene(seed=52 + nf, n_ap=8, pitch=3e-3, nf=nf, n_vox=6, n_pts=20)
     Io, Wo = oracle.full(sc.voxel_centres(), sc.antenna_locs, np.zeros((1, 3)), sc.meas,
                          sc.wavelength, sc.slope)
