@@ -512,7 +512,7 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                 static_assert(T % 2 == 0, "the second-order form takes voxels in pairs");
                 constexpr int L = FORM == kFormMixedClen64 ? 64 : kBlockF;
                 constexpr int LSH = FORM == kFormMixedClen64 ? 6 : 5;
-                const int ns = p.nsmp > 0 ? p.nsmp : fp;  // valid samples per row
+                const int ns = p.nsmp > 0 ? min(p.nsmp, fp) : fp;  // valid samples per row
                 const int nblk_c = ns / L;
                 const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
                 unsigned long long ph[T], stp[T];

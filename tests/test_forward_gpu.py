@@ -299,3 +299,19 @@ def test_every_mixed_variant_edge_cases(cuda_dev, oracle, idx):
         assert oracle.rel_l2(W, Wo) < 1e-4
     finally:
         ops.set_variant("mixed", 0)
+
+
+def test_plan_reports_its_launches(cuda_dev):
+    """mmn_plan_launches: the default (second-order) form reads 16-byte aligned rows of a
+    multiple of 32 samples in place (antenna records + forward kernel), and stages rows of
+    any other length (one more launch), plus the split reduction when the plan splits."""
+    import torch
+    from mmnorm_b200 import ops
+    ops.set_variant("mixed", 0)
+    for nf, want in ((64, 2), (50, 3)):
+        sc = small_scene(seed=70, nf=nf, n_vox=16)
+        args = [_t(v, cuda_dev) for v in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs,
+                                          np.zeros((1, 3), np.float32), sc.meas)]
+        p = ops.make_problem(*args, sc.wavelength, sc.slope)
+        info = ops.plan_info(p, "mixed")
+        assert info["launches"] == want + (1 if info["splits"] > 1 else 0), (nf, info)
