@@ -1012,8 +1012,96 @@ def time_interp(dev, sc, nbins=4096):
                       "path": "reference: pycuda drv.In/Out pattern; ours: mmn_cuda_image from "
                               "the same pageable arrays; host wall clock"}
         out["e2e"]["fast_speedup"] = out["e2e"]["reference_ms"] / out["e2e"]["ours_fast_ms"]
+        del hmr, hmi
+        out["stage_tail"] = time_stage_tail(dev, sc, nbins)
     else:
         out["reference"] = "unavailable: reference cubins not built"
+    return out
+
+
+def reference_stage_tail(x, y, z, locs, radar, rxo, slope, wavelength, bandwidth, S, nbins):
+    """The reference's generate_mmwave_surface_normals tail in interpolated mode
+    (image_processor.py:383-396) with its own CUDA kernels: the zero-padded numpy range FFT
+    (image_processor.py:22-35), image_cuda's host steps (py_image_gpu.py:219-235, 258-302,
+    339-362: re-layout, one group of <= 131072 virtual antennas, per-group mean) around
+    cuda_image with pycuda's per-call transfers, normal_estimates_cuda's
+    (py_sn_est_gpu.py:308-376: mask at 5 % of max|I|, meshgrid voxel lists, NaN scatter)
+    around cuda_sn_est, and the unit normalisation.  Host numpy in and out."""
+    from oracle import ref_cuda
+    A, R = locs.shape[0], rxo.shape[0]
+    assert A * R <= 4096 * 32  # one antenna group, as at this workload
+    pad = np.zeros((A, nbins, R), dtype=np.complex64)
+    pad[:, :S, :] = radar
+    fft = np.fft.fft(pad, axis=1)
+    del pad
+    rows = np.transpose(fft, (0, 2, 1)).reshape(-1, nbins)  # use_4_rx re-layout
+    ant = np.repeat(locs, R, axis=0).astype(np.float32)
+    mr, mi = np.ascontiguousarray(rows.real), np.ascontiguousarray(rows.imag)
+    fsp = np.float32(3e8 / (2 * bandwidth) * S / nbins)
+    nx, ny, nz = len(x), len(y), len(z)
+    p_r, p_i = ref_cuda.cuda_image_in_out(x, y, z, ant.ravel(), mr, mi, rxo.ravel(), slope,
+                                          wavelength, fsp, A * R, R, nbins, 0, 1)
+    image = (p_r.astype(np.float64) + 1j * p_i.astype(np.float64)).reshape(nx, ny, nz) / A
+    filt = np.abs(image) > np.max(np.abs(image)) * 0.05
+    m1, m2, m3 = np.meshgrid(np.arange(ny), np.arange(nx), np.arange(nz))
+    coords = np.concatenate((m2[..., None], m1[..., None], m3[..., None]), axis=-1)[filt]
+    n = ref_cuda.cuda_sn_est_in_out(coords[:, 0], coords[:, 1], coords[:, 2],
+                                    np.real(image).ravel(), np.imag(image).ravel(), x, y, z,
+                                    ant.ravel(), mr, mi, rxo.ravel(), slope, wavelength, fsp,
+                                    A * R, R, nbins, 0)
+    normals = np.full((nx, ny, nz, 3), np.nan)
+    normals[filt] = np.stack(n, axis=1)
+    normals /= np.linalg.norm(normals, axis=-1)[..., np.newaxis].repeat(3, axis=-1)
+    return image, normals
+
+
+def time_stage_tail(dev, sc, nbins):
+    """The whole tail of generate_mmwave_surface_normals in interpolated mode, host arrays
+    in and out: the reference's (numpy FFT + its two CUDA kernels with their per-call
+    transfers + host mask / scatter / normalisation, reference_stage_tail) against
+    stage1.generate_mmwave_surface_normals (range FFT, image and normals on the device), in
+    the bit-exact and the fast form; host wall clock, and the agreement of the outputs."""
+    from mmnorm_b200 import stage1
+    A, S = sc.meas.shape
+    radar = np.ascontiguousarray(sc.meas.reshape(A, S, 1))
+    rxo = np.zeros((1, 3), np.float32)
+    x, y, z = sc.x_locs, sc.y_locs, sc.z_locs
+    locs = np.asarray(sc.antenna_locs, np.float32)
+    wl, sl = np.float32(sc.wavelength), np.float32(sc.slope)
+    bw = sc.f_hi - sc.f_lo
+    ref_out = {}
+
+    def ref():
+        ref_out["r"] = reference_stage_tail(x, y, z, locs, radar, rxo, sl, wl, bw, S, nbins)
+
+    ours_out = {}
+
+    def ours(precision):
+        res = stage1.generate_mmwave_surface_normals(
+            x, y, z, locs, radar, rxo, float(sl), float(wl), bw, S, is_ti_radar=False,
+            use_interpolated_processing=True, precision=precision)
+        ours_out[precision] = res
+
+    ref_ms = min(_wall_ms(ref, reps=2, warm=0))
+    exact_ms = min(_wall_ms(lambda: ours("mixed"), reps=3, warm=1))
+    fast_ms = min(_wall_ms(lambda: ours("fast"), reps=3, warm=1))
+    img_r, nrm_r = ref_out["r"]
+    out = {"what": "generate_mmwave_surface_normals tail, interpolated mode: %d-bin range FFT, "
+                   "image, normals at 5 %% of max|I|, unit normalisation; host arrays in and out"
+                   % nbins,
+           "reference_ms": ref_ms, "ours_exact_ms": exact_ms, "ours_fast_ms": fast_ms,
+           "exact_speedup": ref_ms / exact_ms, "fast_speedup": ref_ms / fast_ms,
+           "reference": "numpy FFT + the reference's cuda_image / cuda_sn_est built from "
+                        "source, pycuda transfer pattern, its host steps"}
+    for key, prec in (("exact", "mixed"), ("fast", "fast")):
+        img_o, _, nrm_o = ours_out[prec][:3]
+        both = np.isfinite(nrm_o).all(-1) & np.isfinite(nrm_r).all(-1)
+        cosang = np.clip(np.sum(nrm_o[both] * nrm_r[both], axis=-1), -1.0, 1.0)
+        out[key + "_vs_reference"] = {
+            "image_rel_l2": float(np.linalg.norm(img_o - img_r) / np.linalg.norm(img_r)),
+            "normal_deg_median": float(np.median(np.degrees(np.arccos(cosang)))),
+            "mask_agreement": float(np.mean(np.isfinite(nrm_o).all(-1) ==
+                                            np.isfinite(nrm_r).all(-1)))}
     return out
 
 

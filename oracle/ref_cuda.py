@@ -141,3 +141,47 @@ def cuda_image_in_out(x, y, z, ant, meas_r, meas_i, rxo, slope, wavelength, fft_
         for d in allocs:
             cu.cuMemFree(d)
     return out_r, out_i
+
+
+def cuda_sn_est_in_out(valid_x, valid_y, valid_z, img_r, img_i, x, y, z, ant, meas_r, meas_i,
+                       rxo, slope, wavelength, fft_spacing, num_ant, num_rx, samples, is_ti):
+    """cuda_sn_est with the reference's per-call transfers (py_sn_est_gpu.py:229-246): the
+    three outputs through drv.Out and every input through drv.In (int32 voxel index lists,
+    float32 arrays), block 512, grid num_valid/512 + 1, start_ind 0, one GPU.  Host numpy
+    in, (n_x, n_y, n_z) float32 numpy out."""
+    import numpy as np
+    import torch
+    from cuda.bindings import driver as cu
+
+    torch.empty(1, device="cuda")  # make the primary context current
+    nx, ny, nz = len(x), len(y), len(z)
+    nv = len(valid_x)
+    allocs = []
+
+    def dev_in(arr, dtype):
+        a = np.ascontiguousarray(arr, dtype=dtype)
+        d = _check(cu.cuMemAlloc(max(4, a.nbytes)), "cuMemAlloc")
+        allocs.append(d)
+        _check(cu.cuMemcpyHtoD(d, a.ctypes.data, a.nbytes), "cuMemcpyHtoD")
+        return _DevPtr(d)
+
+    def dev_out(n):
+        d = _check(cu.cuMemAlloc(max(4, 4 * n)), "cuMemAlloc")
+        allocs.append(d)
+        return _DevPtr(d)
+
+    try:
+        outs = [dev_out(nv) for _ in range(3)]
+        idx = [dev_in(a, np.int32) for a in (valid_x, valid_y, valid_z)]
+        rest = [dev_in(a, np.float32) for a in (img_r, img_i, x, y, z, ant, meas_r, meas_i, rxo)]
+        cuda_sn_est(*outs, *idx, *rest, slope, wavelength, fft_spacing, nx, ny, nz, num_ant,
+                    num_rx, nv, samples, is_ti)
+        res = []
+        for o in outs:
+            h = np.empty(nv, np.float32)
+            _check(cu.cuMemcpyDtoH(h.ctypes.data, o.ptr, 4 * nv), "cuMemcpyDtoH")
+            res.append(h)
+    finally:
+        for d in allocs:
+            cu.cuMemFree(d)
+    return tuple(res)
