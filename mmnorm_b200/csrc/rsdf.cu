@@ -186,6 +186,113 @@ __global__ void bfs_seed_kernel(int32_t seed, int32_t *frontier, uint8_t *visite
     rsdf[seed] = 0.0;
 }
 
+// Small frontiers: one CTA runs whole levels -- the same bids, winners, queue positions
+// and rsdf values as the per-level kernels above, with __syncthreads between the phases
+// instead of kernel boundaries and a host read-back -- until the frontier empties or grows
+// past kSmallFrontier entries (then the per-level kernels take over from the frontier it
+// leaves in global memory).  Each thread owns a run of consecutive slots k = 6 i + d, so
+// a block-wide exclusive scan of the threads' winner counts gives the queue order.  The
+// loop ends: every level marks at least one new voxel of a finite component.
+constexpr int kSmallThreads = 1024;
+constexpr int kSmallFrontier = 4096;  // 24576 slots: at most 24 per thread (one bit each)
+
+struct SmallState {
+    int64_t nf;       // frontier size on exit (0: the search is complete)
+    int64_t visited;  // voxels marked by this launch
+    int32_t parity;   // 1: the exit frontier is in the second buffer
+    int32_t pad;
+};
+
+__global__ void __launch_bounds__(kSmallThreads) bfs_small_kernel(const BfsArgs a, int32_t *fa,
+                                                                  int32_t *fb, int64_t nf0,
+                                                                  SmallState *state) {
+    __shared__ int32_t warp_tot[kSmallThreads / 32];
+    __shared__ int32_t s_total;
+    int32_t *cur = fa, *nxt = fb;
+    int64_t nf = nf0, marked = 0;
+    int32_t parity = 0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    while (nf > 0 && nf <= kSmallFrontier) {
+        const int slots = (int)nf * 6;
+        const int per = (slots + kSmallThreads - 1) / kSmallThreads;
+        const int k0 = tid * per;
+        const int k1 = min(k0 + per, slots);
+        // bids
+        for (int k = k0; k < k1; ++k) {
+            int32_t n;
+            if (neighbour(a, cur[k / 6], k % 6, n) && open_voxel(a, n))
+                atomicMin(&a.bid[n], (unsigned long long)k);
+        }
+        __syncthreads();
+        // winners of this thread's slots
+        uint32_t won = 0;
+        int32_t cnt = 0;
+        for (int k = k0; k < k1; ++k) {
+            int32_t n;
+            // the bids came from atomics at L2 this level: read them past L1
+            if (neighbour(a, cur[k / 6], k % 6, n) && open_voxel(a, n) &&
+                __ldcg(&a.bid[n]) == (unsigned long long)k) {
+                won |= 1u << (k - k0);
+                ++cnt;
+            }
+        }
+        // exclusive scan of the counts over the block, in thread (= slot) order
+        int32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int32_t w = warp_tot[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_tot[lane] = w;  // inclusive over warps
+            if (lane == 31) s_total = w;
+        }
+        __syncthreads();
+        int32_t pos = incl - cnt + (warp > 0 ? warp_tot[warp - 1] : 0);
+        // emit in queue order (the per-level emit kernel's arithmetic)
+        for (int k = k0; k < k1; ++k) {
+            if (!(won >> (k - k0) & 1u)) continue;
+            const int32_t v = cur[k / 6];
+            const int d = k % 6;
+            int32_t n;
+            neighbour(a, v, d, n);
+            const double sx = d == 0 ? -1.0 : (d == 2 ? 1.0 : 0.0);
+            const double sy = d == 1 ? 1.0 : (d == 3 ? -1.0 : 0.0);
+            const double sz = d == 4 ? 1.0 : (d == 5 ? -1.0 : 0.0);
+            const double *nv = a.normals + 3 * (int64_t)n;
+            double acc = 0.0;
+            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(sx, a.dx), nv[0]));
+            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(sy, a.dx), nv[1]));
+            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(sz, a.dx), nv[2]));
+            a.rsdf[n] = __dadd_rn(a.rsdf[v], acc);
+            nxt[pos++] = n;
+        }
+        __syncthreads();
+        const int32_t total = s_total;
+        for (int i = tid; i < total; i += kSmallThreads) a.visited[nxt[i]] = 1;
+        __syncthreads();
+        marked += total;
+        nf = total;
+        int32_t *t = cur;
+        cur = nxt;
+        nxt = t;
+        parity ^= 1;
+    }
+    if (tid == 0) {
+        state->nf = nf;
+        state->visited = marked;
+        state->parity = parity;
+    }
+}
+
 // ---------------------------------------------------------------- exclusive int32 scan
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 4;
@@ -354,8 +461,28 @@ extern "C" int mmn_rsdf_component(int32_t nx, int32_t ny, int32_t nz, const doub
     a.dx = dx;
     bfs_seed_kernel<<<1, 1, 0, stream>>>(seed, fa, visited, rsdf);
     int64_t nf = 1, total = 1;
-    // every level adds at least one voxel, so n levels bound the search
+    // the single-CTA search's exit state, in the workspace header after the status word
+    SmallState *small = reinterpret_cast<SmallState *>(w + 64);
+    // every level (and every single-CTA launch) adds at least one voxel, so n rounds bound
+    // the search
     for (int64_t level = 0; nf > 0 && level <= n; ++level) {
+        if (nf <= kSmallFrontier) {
+            bfs_small_kernel<<<1, kSmallThreads, 0, stream>>>(a, fa, fb, nf, small);
+            SmallState hs;
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(&hs, small, sizeof(hs), cudaMemcpyDeviceToHost, stream) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(stream) != cudaSuccess)
+                return MMN_ERR_CUDA;
+            total += hs.visited;
+            nf = hs.nf;
+            if (hs.parity) {
+                int32_t *t = fa;
+                fa = fb;
+                fb = t;
+            }
+            continue;
+        }
         const int64_t slots = nf * 6;
         bfs_bid_kernel<<<grid_for(slots, 256), 256, 0, stream>>>(a, fa, nf);
         bfs_flag_kernel<<<grid_for(slots, 256), 256, 0, stream>>>(a, fa, nf, flag);

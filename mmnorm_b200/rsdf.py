@@ -63,9 +63,11 @@ def _valid_labels(areas, x_locs):
 def find_connected_components(all_normals, x_locs, _roots=None):
     """(labeled int64 [NX,NY,NZ]: 1 background, 2.. components; valid_labels)."""
     dev = _device()
-    normals = torch.as_tensor(np.asarray(all_normals), device=dev)
-    mask = ~torch.isnan(normals[..., 0])
-    root, count = component_roots(mask) if _roots is None else _roots
+    if _roots is None:
+        normals = torch.as_tensor(np.asarray(all_normals), device=dev)
+        root, count = component_roots(~torch.isnan(normals[..., 0]))
+    else:
+        root, count = _roots
     roots = torch.nonzero(count > 0).flatten()            # ascending: first-voxel order
     lut = torch.zeros(count.numel(), dtype=torch.int64, device=dev)
     lut[roots] = torch.arange(2, roots.numel() + 2, device=dev)
@@ -90,17 +92,43 @@ def _seed(all_normals, coords_full, labeled, component_num):
     return idxs[np.argmin(dists)]
 
 
+def _seed_from_voxels(flat, shape, axes):
+    """_seed for a component given its voxels' flat indices in ascending (C) order: the same
+    coordinate rows, in the same order and dtype, as coords_full[labeled == component], so
+    numpy's mean, norms and argmin -- and the chosen voxel -- are the same."""
+    ny, nz = shape[1], shape[2]
+    ii, rem = np.divmod(flat, ny * nz)
+    jj, kk = np.divmod(rem, nz)
+    x, y, z = axes
+    coords_sel = np.stack([x[ii], y[jj], z[kk]], axis=1)
+    mean_coord = np.mean(coords_sel, axis=0)[None, :]
+    dists = np.linalg.norm((coords_sel - mean_coord), axis=1)
+    return int(flat[np.argmin(dists)])
+
+
+def coordinate_grid(x_locs, y_locs, z_locs):
+    """coords_full of sdf.py:285-287 (the concatenated meshgrid): [NX,NY,NZ,3] with
+    coords[i, j, k] = (x[i], y[j], z[k]), in the meshgrid's dtype, filled by broadcasting."""
+    x, y, z = np.asarray(x_locs), np.asarray(y_locs), np.asarray(z_locs)
+    out = np.empty((len(x), len(y), len(z), 3), dtype=np.result_type(y, x, z))
+    out[..., 0] = x[:, None, None]
+    out[..., 1] = y[None, :, None]
+    out[..., 2] = z[None, None, :]
+    return out
+
+
 def construct_rsdf_components(all_normals, coords_full, labeled, valid_labels, x_locs,
-                              _roots=None):
+                              _roots=None, _normals=None, _axes=None):
     """float64 [NX,NY,NZ]: RSDF on the valid components, NaN elsewhere (sdf.py:122-224)."""
     dev = _device()
     all_normals = np.asarray(all_normals)
     nx, ny, nz = all_normals.shape[:3]
-    normals = torch.as_tensor(np.ascontiguousarray(all_normals, dtype=np.float64), device=dev)
+    normals = _normals if _normals is not None else torch.as_tensor(
+        np.ascontiguousarray(all_normals, dtype=np.float64), device=dev)
     if _roots is None:
-        root, _ = component_roots(~torch.isnan(normals[..., 0]))
+        root, count = component_roots(~torch.isnan(normals[..., 0]))
     else:
-        root = _roots[0]
+        root, count = _roots
     root = root.contiguous()
     rsdf = torch.full((nx, ny, nz), float("nan"), dtype=torch.float64, device=dev)
     lib = _lib.load()
@@ -109,16 +137,26 @@ def construct_rsdf_components(all_normals, coords_full, labeled, valid_labels, x
         raise _lib.MmnError(_lib.MMN_ERR_INVALID_ARGUMENT, "mmn_rsdf_workspace_bytes")
     ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
     dx = float(x_locs[1] - x_locs[0])
+    # with the library's own labels (the roots in ascending order are labels 2, 3, ...),
+    # each component's voxels come from the device and its seed from them alone
+    own = _roots is not None and _axes is not None
+    roots_sorted = torch.nonzero(count > 0).flatten().cpu().numpy() if own else None
+    root_flat = root.reshape(-1)
     root_host = None
     for component_num in valid_labels:
-        i0, j0, k0 = _seed(all_normals, coords_full, labeled, component_num)
-        if root_host is None:
-            root_host = root.cpu().numpy()
-        comp_root = int(root_host[i0, j0, k0])
-        seed = int((i0 * ny + j0) * nz + k0)
-        count = ctypes.c_int64(0)
+        if own:
+            comp_root = int(roots_sorted[component_num - 2])
+            flat = torch.nonzero(root_flat == comp_root).flatten().cpu().numpy()
+            seed = _seed_from_voxels(flat, (nx, ny, nz), _axes)
+        else:
+            i0, j0, k0 = _seed(all_normals, coords_full, labeled, component_num)
+            if root_host is None:
+                root_host = root.cpu().numpy()
+            comp_root = int(root_host[i0, j0, k0])
+            seed = int((i0 * ny + j0) * nz + k0)
+        count_v = ctypes.c_int64(0)
         _lib.check(lib.mmn_rsdf_component(nx, ny, nz, _vp(normals), _vp(root), comp_root, seed,
-                                          dx, _vp(rsdf), ctypes.byref(count), _vp(ws), nbytes,
+                                          dx, _vp(rsdf), ctypes.byref(count_v), _vp(ws), nbytes,
                                           _stream(dev)), "mmn_rsdf_component")
     return rsdf.cpu().numpy()
 
@@ -126,13 +164,12 @@ def construct_rsdf_components(all_normals, coords_full, labeled, valid_labels, x
 def compute_rsdf(all_normals, x_locs, y_locs, z_locs):
     """Steps 2-3 of compute_rsdf (sdf.py:285-289) on normals already masked by the binary
     image and normalised: (rsdf, labeled, valid_labels, coords_full)."""
-    mesh1, mesh2, mesh3 = np.meshgrid(y_locs, x_locs, z_locs)
-    coords_full = np.concatenate((mesh2[..., np.newaxis], mesh1[..., np.newaxis],
-                                  mesh3[..., np.newaxis]), axis=-1)
+    coords_full = coordinate_grid(x_locs, y_locs, z_locs)
     dev = _device()
     normals = torch.as_tensor(np.ascontiguousarray(all_normals, dtype=np.float64), device=dev)
     roots = component_roots(~torch.isnan(normals[..., 0]))
     labeled, valid = find_connected_components(all_normals, x_locs, _roots=roots)
+    axes = (np.asarray(x_locs), np.asarray(y_locs), np.asarray(z_locs))
     rsdf = construct_rsdf_components(all_normals, coords_full, labeled, valid, x_locs,
-                                     _roots=roots)
+                                     _roots=roots, _normals=normals, _axes=axes)
     return rsdf, labeled, valid, coords_full
