@@ -65,10 +65,23 @@ def test_accuracy_workload_subset(cuda_dev, oracle, sign):
     for mode in ("mixed", "plain"):
         I, W = _run(cuda_dev, sc, mode)
         out[mode] = _stats(oracle, I, W, idx, Io, Wo)
+    # "mixed" runs the default variant (second order, 32-sample blocks); also the variant
+    # the autotuner picks on this workload and the first-order Horner form
+    from mmnorm_b200 import ops
+    names = [v["name"] for v in ops.variants("mixed")]
+    out["mixed_variants"] = {}
+    try:
+        for name in ("mixed_clen64_fx2_t4_n128_s24", "mixed_antpair_fx2_t1_n256"):
+            ops.set_variant("mixed", names.index(name))
+            I, W = _run(cuda_dev, sc, "mixed")
+            out["mixed_variants"][name] = _stats(oracle, I, W, idx, Io, Wo)
+    finally:
+        ops.set_variant("mixed", 0)
     _report("accuracy_%s_sign%+d" % (sc.name, sign), out)
-    assert out["mixed"]["image_rel_l2"] <= 1e-4
-    assert out["mixed"]["vote_rel_l2"] <= 1e-4
-    assert out["mixed"]["normal_deg_median"] <= 0.5
+    for r in [out["mixed"]] + list(out["mixed_variants"].values()):
+        assert r["image_rel_l2"] <= 1e-4
+        assert r["vote_rel_l2"] <= 1e-4
+        assert r["normal_deg_median"] <= 0.5
 
 
 def test_accuracy_full_grid_64(cuda_dev, oracle):
