@@ -110,30 +110,45 @@ __device__ __forceinline__ void clen_block(const float4 *mb, bool clen, const fl
             si[k] = fmaf(-zr[k], b2[k].y, fmaf(zi[k], b2[k].x, b1[k].y));
         }
     } else {
-        // first-order Horner, h <- h z + m_t
+        // first-order Horner, h <- h z + m_t, voxel pairs in the halves of FFMA2 (each half
+        // rounds as the scalar FMA: the same bits as the scalar form)
+        constexpr int P = T / 2;
+        float2 hr[P], hi[P], zr2[P], zi2[P], nzi2[P];
 #pragma unroll
-        for (int k = 0; k < T; ++k) {
-            sr[k] = top.z;
-            si[k] = top.w;
-            const float u = fmaf(sr[k], zr[k], top.x);
-            const float w = fmaf(sr[k], zi[k], top.y);
-            sr[k] = fmaf(-si[k], zi[k], u);
-            si[k] = fmaf(si[k], zr[k], w);
+        for (int q = 0; q < P; ++q) {
+            zr2[q] = make_float2(zr[2 * q], zr[2 * q + 1]);
+            zi2[q] = make_float2(zi[2 * q], zi[2 * q + 1]);
+            nzi2[q] = make_float2(-zi[2 * q], -zi[2 * q + 1]);
+            hr[q] = make_float2(top.z, top.z);
+            hi[q] = make_float2(top.w, top.w);
+            const float2 u = __ffma2_rn(hr[q], zr2[q], make_float2(top.x, top.x));
+            const float2 w = __ffma2_rn(hr[q], zi2[q], make_float2(top.y, top.y));
+            hr[q] = __ffma2_rn(hi[q], nzi2[q], u);
+            hi[q] = __ffma2_rn(hi[q], zr2[q], w);
         }
 #pragma unroll 1
-        for (int q = L / 2 - 2; q >= 0; --q) {
-            const float4 mm = mb[q];
+        for (int q2 = L / 2 - 2; q2 >= 0; --q2) {
+            const float4 mm = mb[q2];
+            const float2 m1r = make_float2(mm.z, mm.z), m1i = make_float2(mm.w, mm.w);
+            const float2 m0r = make_float2(mm.x, mm.x), m0i = make_float2(mm.y, mm.y);
 #pragma unroll
-            for (int k = 0; k < T; ++k) {
-                float u = fmaf(sr[k], zr[k], mm.z);
-                float w = fmaf(sr[k], zi[k], mm.w);
-                sr[k] = fmaf(-si[k], zi[k], u);
-                si[k] = fmaf(si[k], zr[k], w);
-                u = fmaf(sr[k], zr[k], mm.x);
-                w = fmaf(sr[k], zi[k], mm.y);
-                sr[k] = fmaf(-si[k], zi[k], u);
-                si[k] = fmaf(si[k], zr[k], w);
+            for (int q = 0; q < P; ++q) {
+                float2 u = __ffma2_rn(hr[q], zr2[q], m1r);
+                float2 w = __ffma2_rn(hr[q], zi2[q], m1i);
+                hr[q] = __ffma2_rn(hi[q], nzi2[q], u);
+                hi[q] = __ffma2_rn(hi[q], zr2[q], w);
+                u = __ffma2_rn(hr[q], zr2[q], m0r);
+                w = __ffma2_rn(hr[q], zi2[q], m0i);
+                hr[q] = __ffma2_rn(hi[q], nzi2[q], u);
+                hi[q] = __ffma2_rn(hi[q], zr2[q], w);
             }
+        }
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            sr[2 * q] = hr[q].x;
+            sr[2 * q + 1] = hr[q].y;
+            si[2 * q] = hi[q].x;
+            si[2 * q + 1] = hi[q].y;
         }
     }
 }
