@@ -1019,22 +1019,26 @@ def time_interp(dev, sc, nbins=4096):
     return out
 
 
-def reference_stage_tail(x, y, z, locs, radar, rxo, slope, wavelength, bandwidth, S, nbins):
-    """The reference's generate_mmwave_surface_normals tail in interpolated mode
-    (image_processor.py:383-396) with its own CUDA kernels: the zero-padded numpy range FFT
-    (image_processor.py:22-35), image_cuda's host steps (py_image_gpu.py:219-235, 258-302,
-    339-362: re-layout, one group of <= 131072 virtual antennas, per-group mean) around
-    cuda_image with pycuda's per-call transfers, normal_estimates_cuda's
-    (py_sn_est_gpu.py:308-376: mask at 5 % of max|I|, meshgrid voxel lists, NaN scatter)
-    around cuda_sn_est, and the unit normalisation.  Host numpy in and out."""
-    from oracle import ref_cuda
-    A, R = locs.shape[0], rxo.shape[0]
-    assert A * R <= 4096 * 32  # one antenna group, as at this workload
+def range_fft_host(radar, nbins):
+    """ImageProcessor.interpolate_measurements (image_processor.py:22-35): zero-pad the
+    samples to nbins and FFT along the sample axis with numpy."""
+    A, S, R = radar.shape
     pad = np.zeros((A, nbins, R), dtype=np.complex64)
     pad[:, :S, :] = radar
-    fft = np.fft.fft(pad, axis=1)
-    del pad
-    rows = np.transpose(fft, (0, 2, 1)).reshape(-1, nbins)  # use_4_rx re-layout
+    return np.fft.fft(pad, axis=1)
+
+
+def reference_dropin_calls(x, y, z, locs, bins, rxo, slope, wavelength, bandwidth, S):
+    """image_processor.py:390-396 with the reference's own CUDA kernels: image_cuda's host
+    steps (py_image_gpu.py:219-235, 258-302, 339-362: use_4_rx re-layout, one group of
+    <= 131072 virtual antennas, per-group mean) around cuda_image with pycuda's per-call
+    transfers, normal_estimates_cuda's (py_sn_est_gpu.py:308-376: mask at 5 % of max|I|,
+    meshgrid voxel lists, NaN scatter) around cuda_sn_est, and the unit normalisation.
+    Host numpy in and out."""
+    from oracle import ref_cuda
+    A, nbins, R = bins.shape
+    assert A * R <= 4096 * 32  # one antenna group, as at this workload
+    rows = np.transpose(bins, (0, 2, 1)).reshape(-1, nbins)  # use_4_rx re-layout
     ant = np.repeat(locs, R, axis=0).astype(np.float32)
     mr, mi = np.ascontiguousarray(rows.real), np.ascontiguousarray(rows.imag)
     fsp = np.float32(3e8 / (2 * bandwidth) * S / nbins)
@@ -1056,12 +1060,15 @@ def reference_stage_tail(x, y, z, locs, radar, rxo, slope, wavelength, bandwidth
 
 
 def time_stage_tail(dev, sc, nbins):
-    """The whole tail of generate_mmwave_surface_normals in interpolated mode, host arrays
-    in and out: the reference's (numpy FFT + its two CUDA kernels with their per-call
-    transfers + host mask / scatter / normalisation, reference_stage_tail) against
-    stage1.generate_mmwave_surface_normals (range FFT, image and normals on the device), in
-    the bit-exact and the fast form; host wall clock, and the agreement of the outputs."""
-    from mmnorm_b200 import stage1
+    """The whole tail of generate_mmwave_surface_normals in interpolated mode
+    (image_processor.py:383-396), host arrays in and out, three ways: the reference's
+    (numpy range FFT + reference_dropin_calls: its two CUDA kernels with their per-call
+    transfers and its host steps); the same numpy FFT followed by this library's drop-in
+    image_cuda / normal_estimates_cuda in their place (what swapping the two imports at
+    image_processor.py:10-14 gives); and stage1.generate_mmwave_surface_normals (range FFT,
+    image and normals on the device).  Bit-exact and fast forms; host wall clock, and the
+    agreement of the outputs with the reference's."""
+    from mmnorm_b200 import py_image_gpu, py_sn_est_gpu, stage1
     A, S = sc.meas.shape
     radar = np.ascontiguousarray(sc.meas.reshape(A, S, 1))
     rxo = np.zeros((1, 3), np.float32)
@@ -1069,32 +1076,49 @@ def time_stage_tail(dev, sc, nbins):
     locs = np.asarray(sc.antenna_locs, np.float32)
     wl, sl = np.float32(sc.wavelength), np.float32(sc.slope)
     bw = sc.f_hi - sc.f_lo
-    ref_out = {}
+    res = {}
 
     def ref():
-        ref_out["r"] = reference_stage_tail(x, y, z, locs, radar, rxo, sl, wl, bw, S, nbins)
+        bins = range_fft_host(radar, nbins)
+        res["ref"] = reference_dropin_calls(x, y, z, locs, bins, rxo, sl, wl, bw, S)
 
-    ours_out = {}
+    def dropin(precision):
+        bins = range_fft_host(radar, nbins)
+        img, _ = py_image_gpu.image_cuda(x, y, z, locs, bins, rxo, float(sl), float(wl), bw, S,
+                                         use_4_rx=True, use_interpolated_processing=True,
+                                         precision=precision)
+        nrm = py_sn_est_gpu.normal_estimates_cuda(img, x, y, z, locs, bins, rxo, float(sl),
+                                                  float(wl), bw, S, use_4_rx=True,
+                                                  precision=precision)
+        nrm /= np.linalg.norm(nrm, axis=-1)[..., np.newaxis].repeat(3, axis=-1)
+        res["dropin_" + precision] = (img, nrm)
 
     def ours(precision):
-        res = stage1.generate_mmwave_surface_normals(
+        out = stage1.generate_mmwave_surface_normals(
             x, y, z, locs, radar, rxo, float(sl), float(wl), bw, S, is_ti_radar=False,
             use_interpolated_processing=True, precision=precision)
-        ours_out[precision] = res
+        res["stage1_" + precision] = (out[0], out[2])
 
+    fft_ms = min(_wall_ms(lambda: range_fft_host(radar, nbins), reps=2, warm=0))
     ref_ms = min(_wall_ms(ref, reps=2, warm=0))
-    exact_ms = min(_wall_ms(lambda: ours("mixed"), reps=3, warm=1))
-    fast_ms = min(_wall_ms(lambda: ours("fast"), reps=3, warm=1))
-    img_r, nrm_r = ref_out["r"]
     out = {"what": "generate_mmwave_surface_normals tail, interpolated mode: %d-bin range FFT, "
                    "image, normals at 5 %% of max|I|, unit normalisation; host arrays in and out"
                    % nbins,
-           "reference_ms": ref_ms, "ours_exact_ms": exact_ms, "ours_fast_ms": fast_ms,
-           "exact_speedup": ref_ms / exact_ms, "fast_speedup": ref_ms / fast_ms,
+           "reference_ms": ref_ms, "numpy_fft_ms": fft_ms,
            "reference": "numpy FFT + the reference's cuda_image / cuda_sn_est built from "
                         "source, pycuda transfer pattern, its host steps"}
-    for key, prec in (("exact", "mixed"), ("fast", "fast")):
-        img_o, _, nrm_o = ours_out[prec][:3]
+    for key, prec in (("exact", "exact"), ("fast", "fast")):
+        out["dropin_%s_ms" % key] = min(_wall_ms(lambda: dropin(prec), reps=2, warm=1))
+    out["ours_exact_ms"] = min(_wall_ms(lambda: ours("mixed"), reps=3, warm=1))
+    out["ours_fast_ms"] = min(_wall_ms(lambda: ours("fast"), reps=3, warm=1))
+    for k in ("dropin_exact", "dropin_fast", "ours_exact", "ours_fast"):
+        out[k.replace("ours", "stage1") + "_speedup" if k.startswith("ours") else
+            k + "_speedup"] = ref_ms / out[k + "_ms"]
+    out["exact_speedup"], out["fast_speedup"] = (out["stage1_exact_speedup"],
+                                                 out["stage1_fast_speedup"])
+    img_r, nrm_r = res["ref"]
+    for key in ("dropin_exact", "dropin_fast", "stage1_mixed", "stage1_fast"):
+        img_o, nrm_o = res[key]
         both = np.isfinite(nrm_o).all(-1) & np.isfinite(nrm_r).all(-1)
         cosang = np.clip(np.sum(nrm_o[both] * nrm_r[both], axis=-1), -1.0, 1.0)
         out[key + "_vs_reference"] = {

@@ -58,7 +58,9 @@ def _rows(measurements, samples_per_meas, num_ant):
     if measurements.size < need:
         raise ValueError("radar_data holds %d samples, the antenna list needs %d"
                          % (measurements.size, need))
-    return np.ascontiguousarray(measurements[:need].astype(np.complex64)).reshape(
+    # no copy when the caller's samples are already contiguous complex64 (numpy >= 2 keeps
+    # complex64 through np.fft, so the range-FFT bins of interpolated mode arrive that way)
+    return np.ascontiguousarray(measurements[:need].astype(np.complex64, copy=False)).reshape(
         num_ant, samples_per_meas)
 
 

@@ -62,8 +62,10 @@ def sn_est_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_
     if measurements.size < need:
         raise ValueError("radar_data holds %d samples, the antenna list needs %d"
                          % (measurements.size, need))
-    meas_r = np.ascontiguousarray(measurements[:need].real, dtype=np.float32)
-    meas_i = np.ascontiguousarray(measurements[:need].imag, dtype=np.float32)
+    # one host-to-device copy of the complex samples; the float32 real / imaginary planes
+    # the kernel reads are split on the device
+    meas_dev = torch.as_tensor(np.ascontiguousarray(measurements[:need]).astype(
+        np.complex64, copy=False), device=dev)
     sum_image = np.asarray(sum_image)
     filter_idx, coords = _mask_and_coords(sum_image, initial_filter_percent)
     num_x, num_y, num_z = len(x_locs), len(y_locs), len(z_locs)
@@ -80,11 +82,13 @@ def sn_est_cuda(sum_image, x_locs, y_locs, z_locs, antenna_locs, radar_data, rx_
         vx=ti32(coords[:, 0]), vy=ti32(coords[:, 1]), vz=ti32(coords[:, 2]),
         ir=t32(np.real(sum_image).reshape(-1)), ii=t32(np.imag(sum_image).reshape(-1)),
         x=t32(x_locs), y=t32(y_locs), z=t32(z_locs),
-        ant=t32(np.asarray(antenna_locs).reshape(-1)), mr=t32(meas_r), mi=t32(meas_i),
+        ant=t32(np.asarray(antenna_locs).reshape(-1)), mr=meas_dev.real.contiguous(),
+        mi=meas_dev.imag.contiguous(),
         rxo=t32(np.asarray(rx_offset_flat).reshape(-1)),
         nx=torch.zeros(nvalid, dtype=torch.float32, device=dev),
         ny=torch.zeros(nvalid, dtype=torch.float32, device=dev),
         nz=torch.zeros(nvalid, dtype=torch.float32, device=dev))
+    del meas_dev
     ws_bytes = max(256, _lib.load().mmn_cuda_sn_est_workspace_bytes(num_ant, samples_per_meas))
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     vp = ops._vp
