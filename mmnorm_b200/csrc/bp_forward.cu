@@ -51,7 +51,7 @@ constexpr int kFormMixedAntPair = 3; // FFMA2 antenna pairs, (re_a,re_a',im_a,im
 constexpr int kFormMixedPairSplit = 4;
 // second-order (Clenshaw) form of the block sum, (re, im) samples: see fwd_item
 constexpr int kFormMixedClen = 5;
-constexpr int kFormMixedClen64 = 6;  // the same with 64-sample blocks (+ a last 32 if needed)
+constexpr int kFormMixedClen64 = 6;  // the same with 64-sample blocks
 // The second-order form is used for a warp's (voxels, antenna) pairs when every lane's
 // per-sample rotation z = e^{-i theta} has |cos theta| <= kClenMaxCos (theta in
 // [0.2, pi - 0.2]); otherwise that antenna's blocks run the first-order Horner form.
@@ -515,8 +515,8 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                 // so each (voxel, antenna) chain keeps its complex b as one (re, im) register
                 // pair: one FADD2 + one FFMA2 per sample (4 lane operations, as the Horner step),
                 // and one 16-byte shared load feeds two samples to every voxel of the thread.
-                // Blocks are L = 32 or 64 samples long (kFormMixedClen64: half the re-anchoring;
-                // rows are padded to 32 samples, a last half block runs with L = 32).
+                // Blocks are L = 32 or 64 samples long (kFormMixedClen64: half the re-anchoring);
+                // a row's last block runs over its remaining valid samples only.
                 // Error: a rounding error made at step t reaches b_0 scaled by at most
                 // min(t + 1, 1 / |sin phi|), and for rows dominated by a few scatterers (input
                 // near the recurrence's own modes e^{+-i phi t}) |b| grows to ~L|m| / sin phi,
@@ -548,8 +548,8 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                     }
 #pragma unroll
                     for (int q = 0; q < T / 2; ++q) {
-                        float2 c, s, ns;
-                        cis_turns_pair(za[2 * q], za[2 * q + 1], c, s, ns);
+                        float2 c, s, nsn;
+                        cis_turns_pair(za[2 * q], za[2 * q + 1], c, s, nsn);
                         zr[2 * q] = c.x;
                         zr[2 * q + 1] = c.y;
                         zi[2 * q] = s.x;
