@@ -50,3 +50,24 @@ def reference_dropin_calls(x, y, z, locs, bins, rxo, slope, wavelength, bandwidt
     normals[filt] = np.stack(n, axis=1)
     normals /= np.linalg.norm(normals, axis=-1)[..., np.newaxis].repeat(3, axis=-1)
     return image, normals
+
+
+def reference_full_image(x, y, z, locs, radar, rxo, slope, wavelength, bandwidth, S,
+                         is_ti=0):
+    """py_image_gpu.image_cuda in full matched-filter mode (py_image_gpu.py:308-336) with
+    the reference's cuda_image: use_4_rx re-layout, the kernel's full branch, the division
+    by the TX count in _run_cuda_image (:302) and again in image_cuda (:330), and the
+    virtual phase centres (:332-336).  Host numpy in and out."""
+    A, _, R = radar.shape
+    rows = np.transpose(radar, (0, 2, 1)).reshape(-1, S)
+    ant = np.repeat(locs, R, axis=0).astype(np.float32)
+    mr, mi = np.ascontiguousarray(rows.real), np.ascontiguousarray(rows.imag)
+    fsp = np.float32(3e8 / (2 * bandwidth) * S / S)
+    nx, ny, nz = len(x), len(y), len(z)
+    p_r, p_i = ref_cuda.cuda_image_in_out(x, y, z, ant.ravel(), mr, mi, rxo.ravel(), slope,
+                                          wavelength, fsp, A * R, R, S, is_ti, 0)
+    image = (p_r.astype(np.float64) + 1j * p_i.astype(np.float64)).reshape(nx, ny, nz) / A
+    image = image / A
+    rep = np.tile(rxo, reps=(len(ant) // len(rxo), 1))
+    centres = (ant + (ant + rep)) / 2
+    return image, centres

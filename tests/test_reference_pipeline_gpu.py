@@ -73,3 +73,25 @@ def test_dropin_tail_matches_reference(cuda_dev, ref_pipeline, rx, is_ti):
             both = fin_o & fin_r
             cosang = np.clip(np.sum(nrm[both] * nrm_r[both], axis=-1), -1.0, 1.0)
             assert np.median(np.degrees(np.arccos(cosang))) < 1e-3
+
+
+@pytest.mark.parametrize("rx,is_ti", [(1, 0), (4, 1)])
+def test_dropin_full_mode_image_matches_reference(cuda_dev, ref_pipeline, rx, is_ti):
+    """Full matched filter through image_cuda: the reference's cuda_image (FP32 range and
+    phase, FP64 sin/cos) behind its host steps against the drop-in's mixed-precision
+    kernel behind the same contract (/A twice, complex image, phase centres).  The forms
+    differ by the reference's FP32 range error (~3e-5 relative; bound 2e-4)."""
+    from mmnorm_b200 import py_image_gpu
+    sc, radar, rxo = _case(rx, is_ti)
+    A, S, R = radar.shape
+    locs = np.asarray(sc.antenna_locs, np.float32)
+    wl, sl, bw = np.float32(sc.wavelength), np.float32(sc.slope), sc.f_hi - sc.f_lo
+    img_r, cen_r = ref_pipeline.reference_full_image(sc.x_locs, sc.y_locs, sc.z_locs, locs,
+                                                     radar, rxo, sl, wl, bw, S, is_ti)
+    img, cen = py_image_gpu.image_cuda(sc.x_locs, sc.y_locs, sc.z_locs, locs, radar, rxo,
+                                       float(sl), float(wl), bw, S, use_4_rx=True,
+                                       is_ti_radar=bool(is_ti),
+                                       use_interpolated_processing=False)
+    rel = np.linalg.norm(img - img_r) / np.linalg.norm(img_r)
+    assert rel < 2e-4, rel
+    assert np.allclose(cen, cen_r, rtol=0, atol=1e-7)
