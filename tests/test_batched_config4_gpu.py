@@ -23,7 +23,16 @@ def test_config4_batch_vs_individual_and_oracle(cuda_dev, oracle):
     objs = [dict(x_locs=t(sc.x_locs), y_locs=t(sc.y_locs), z_locs=t(sc.z_locs),
                  antenna_locs=t(sc.antenna_locs), rx_offsets=t(np.zeros((1, 3), np.float32)),
                  meas=t(sc.meas), wavelength=sc.wavelength, slope=sc.slope) for sc in scs]
-    tuned = autotune.tune_batched(objs)
+    previous = ops.current_variant("mixed")
+    try:
+        _check(cuda_dev, oracle, scs, objs, autotune.tune_batched(objs))
+    finally:  # the batched tuner makes its variant current: leave the process as found
+        ops.set_variant("mixed", previous)
+
+
+def _check(cuda_dev, oracle, scs, objs, tuned):
+    import torch
+    from mmnorm_b200 import ops
     plan = ops.BatchPlan(objs, items_per_slot=tuned["best"])
     plan.capture()
     for _ in range(2):  # two replays: the second must not depend on the first's leftovers
