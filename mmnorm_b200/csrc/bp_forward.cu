@@ -18,11 +18,13 @@
 // phase
 //     c_i += exp(-j d kappa_{L b}) * h_b,   h_b = sum_{t<L} m[i, L b + t] * z^t.
 // The per-sample work is 4 FP32 lane operations, no SFU, in one of two recurrences:
-//  * second-order (Clenshaw) -- the default variant and the autotuner's usual pick:
+//  * second-order (Clenshaw) -- the autotuner's usual pick:
 //    b_t = m_t + 2 cos(theta) b_{t+1} - b_{t+2}, h_b = b_0 - conj(z) b_1.  The multiplier
 //    is real, so a (voxel, antenna) chain is one (re, im) register pair: one FADD2 + one
 //    FFMA2 (Blackwell's packed FP32) per sample on plain (re, im) samples, one 16-byte
-//    shared load feeding two samples to each of the thread's voxels;
+//    shared load feeding two samples to each of the thread's voxels.  The default variant
+//    splits each 64-sample block into even and odd chains in z^2 (clen_block_eo), which
+//    keeps the second-order form's extra error small at a few per cent of its speed;
 //  * first-order Horner, h <- h z + m_t (one complex multiply-add): voxel pairs or
 //    antenna pairs in the halves of FFMA2 (the sample duplicated into (re, re, im, im)
 //    or antenna-pair records), or scalar FFMA.
@@ -52,6 +54,8 @@ constexpr int kFormMixedPairSplit = 4;
 // second-order (Clenshaw) form of the block sum, (re, im) samples: see fwd_item
 constexpr int kFormMixedClen = 5;
 constexpr int kFormMixedClen64 = 6;  // the same with 64-sample blocks
+// 64-sample blocks as two interleaved second-order chains in z^2 (clen_block_eo)
+constexpr int kFormMixedClenEO = 7;
 // The second-order form is used for a warp's (voxels, antenna) pairs when every lane's
 // per-sample rotation z = e^{-i theta} has |cos theta| <= kClenMaxCos (theta in
 // [0.2, pi - 0.2]); otherwise that antenna's blocks run the first-order Horner form.
@@ -150,6 +154,54 @@ __device__ __forceinline__ void clen_block(const float4 *mb, bool clen, const fl
             si[2 * q] = hi[q].x;
             si[2 * q + 1] = hi[q].y;
         }
+    }
+}
+
+// A 64-sample block of the split second-order form (kFormMixedClenEO): the even and the
+// odd samples as two chains in w = z^2, E = sum_k m_{2k} w^k and O = sum_k m_{2k+1} w^k,
+// each by Clenshaw's recurrence with the real multiplier c2w = 2 cos(2 phi), and
+// h = E + z O.  One 16-byte load (samples 2k, 2k+1) feeds one step of both chains; the
+// chains are half as long and their modes e^{+-2 i phi} twice as far from 0, which keeps
+// the growth of b and the effect of the FP32 multiplier's rounding several times smaller
+// than one chain over the whole block.
+template <int T>
+__device__ __forceinline__ void clen_block_eo(const float4 *mb, const float (&zr)[T],
+                                              const float (&zi)[T], const float (&wr)[T],
+                                              const float (&wi)[T], float (&sr)[T],
+                                              float (&si)[T]) {
+    const float4 top = mb[31];  // samples 62 (even k = 31), 63 (odd k = 31)
+    float2 be1[T], be2[T], bo1[T], bo2[T], c2[T];
+#pragma unroll
+    for (int k = 0; k < T; ++k) {
+        c2[k] = make_float2(2.f * wr[k], 2.f * wr[k]);
+        be1[k] = make_float2(top.x, top.y);  // b_31 of each chain
+        bo1[k] = make_float2(top.z, top.w);
+        be2[k] = bo2[k] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 30; q >= 0; --q) {
+        const float4 mm = mb[q];
+#pragma unroll
+        for (int k = 0; k < T; ++k) {
+            const float2 de = __fadd2_rn(make_float2(mm.x, mm.y),
+                                         make_float2(-be2[k].x, -be2[k].y));
+            const float2 dd = __fadd2_rn(make_float2(mm.z, mm.w),
+                                         make_float2(-bo2[k].x, -bo2[k].y));
+            be2[k] = be1[k];
+            bo2[k] = bo1[k];
+            be1[k] = __ffma2_rn(c2[k], be1[k], de);
+            bo1[k] = __ffma2_rn(c2[k], bo1[k], dd);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < T; ++k) {
+        // E = b0 - conj(w) b1 for each chain, then h = E + z O
+        const float er = fmaf(-wr[k], be2[k].x, fmaf(-wi[k], be2[k].y, be1[k].x));
+        const float ei = fmaf(-wr[k], be2[k].y, fmaf(wi[k], be2[k].x, be1[k].y));
+        const float orr = fmaf(-wr[k], bo2[k].x, fmaf(-wi[k], bo2[k].y, bo1[k].x));
+        const float oi = fmaf(-wr[k], bo2[k].y, fmaf(wi[k], bo2[k].x, bo1[k].y));
+        sr[k] = fmaf(zr[k], orr, fmaf(-zi[k], oi, er));
+        si[k] = fmaf(zr[k], oi, fmaf(zi[k], orr, ei));
     }
 }
 
@@ -588,6 +640,74 @@ __device__ __forceinline__ int fwd_item(const FwdParams &p, int tile, int split,
                                     sr, si);
                     anchor(sr, si, 0);
                 }
+            } else if constexpr (FORM == kFormMixedClenEO) {
+                // 64-sample blocks, each as even and odd chains in w = z^2 (clen_block_eo),
+                // used for a warp's antenna when every lane has |cos 2 phi| <= kClenMaxCos;
+                // otherwise, and for a row's last partial block, first-order Horner.
+                static_assert(T % 2 == 0, "the second-order form takes voxels in pairs");
+                const int ns = p.nsmp > 0 ? min(p.nsmp, fp) : fp;
+                const int nblk_c = ns / 64;
+                const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
+                unsigned long long ph[T], stp[T];
+                float zr[T], zi[T], wr[T], wi[T];
+                bool eo = true;
+                {
+                    int32_t za[T], wa[T];
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        const double d = range_fp64_newton((double)vx[k], (double)vy[k],
+                                                           (double)vz[k], ar, mono, p.ti);
+                        const unsigned long long u = turns_fixed64(-d * p.tsmp);
+                        za[k] = (int32_t)(u >> 32);
+                        wa[k] = (int32_t)((u << 1) >> 32);  // 2 phi, exact in fixed point
+                        stp[k] = u << 6;
+                        ph[k] = turns_fixed_top(-d * p.t0);
+                        cr[k] = ci[k] = 0.f;
+                    }
+#pragma unroll
+                    for (int q = 0; q < T / 2; ++q) {
+                        float2 c, s, nsn;
+                        cis_turns_pair(za[2 * q], za[2 * q + 1], c, s, nsn);
+                        zr[2 * q] = c.x;
+                        zr[2 * q + 1] = c.y;
+                        zi[2 * q] = s.x;
+                        zi[2 * q + 1] = s.y;
+                        cis_turns_pair(wa[2 * q], wa[2 * q + 1], c, s, nsn);
+                        wr[2 * q] = c.x;
+                        wr[2 * q + 1] = c.y;
+                        wi[2 * q] = s.x;
+                        wi[2 * q + 1] = s.y;
+                    }
+#pragma unroll
+                    for (int k = 0; k < T; ++k) eo = eo && fabsf(wr[k]) <= kClenMaxCos;
+                }
+                eo = __all_sync(0xffffffffu, eo);
+                const float2 none[T] = {};
+                auto anchor = [&](const float (&sr)[T], const float (&si)[T]) {
+#pragma unroll
+                    for (int k = 0; k < T; ++k) {
+                        float anr, ani;
+                        fixed_cis(ph[k], anr, ani);
+                        ph[k] += stp[k];
+                        cr[k] = fmaf(anr, sr[k], fmaf(-ani, si[k], cr[k]));
+                        ci[k] = fmaf(anr, si[k], fmaf(ani, sr[k], ci[k]));
+                    }
+                };
+                for (int b = 0; b < nblk_c; ++b) {
+                    float sr[T], si[T];
+                    if (eo)
+                        clen_block_eo<T>(m4 + b * 32, zr, zi, wr, wi, sr, si);
+                    else
+                        clen_block<T, 64>(m4 + b * 32, false, none, zr, zi, sr, si);
+                    anchor(sr, si);
+                }
+                const int rem = ns - nblk_c * 64;
+                if (rem > 0) {
+                    float sr[T], si[T];
+                    clen_partial<T>(reinterpret_cast<const float2 *>(m4 + nblk_c * 32), rem,
+                                    false, none, zr, zi, sr, si);
+                    anchor(sr, si);
+                }
             } else if constexpr (FORM == kFormMixedScalar) {
                 const float4 *m4 = reinterpret_cast<const float4 *>(mstage) + (size_t)a * (fp / 2);
                 double d[T];
@@ -858,7 +978,9 @@ static const void *pers_ptr() {
 const FwdVariant *fwd_variants(int *count) {
     // index order: the MIXED variants first (default first), then the PLAIN ones
     static const FwdVariant v[] = {
-        // default: second-order block sums, 32-sample blocks, 4 voxels per thread
+        // default: 64-sample blocks as two second-order chains in z^2 (near the Horner
+        // form's accuracy at close to the fastest form's speed)
+        {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClenEO, kAnchorFixed2>(), "mixed_clen64eo_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClenEO, kAnchorFixed2>()},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), "mixed_clen_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen, kAnchorFixed2>(), 24 * 1024},
         {2, 256, false, 16, fwd_ptr<2, 256, kFormMixedPair, kAnchorFixed>(), "mixed_ffma2_fx_t2_n256", 1, pers_ptr<2, 256, kFormMixedPair, kAnchorFixed>()},
         // each block as two 16-step chains joined by z^16 (kFormMixedPairSplit)
@@ -903,6 +1025,8 @@ const FwdVariant *fwd_variants(int *count) {
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), 24 * 1024},
         {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t4_n128", 0, pers_ptr<4, 128, kFormMixedClen64, kAnchorFixed2>()},
         {2, 256, false, 8, fwd_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>(), "mixed_clen64_fx2_t2_n256", 0, pers_ptr<2, 256, kFormMixedClen64, kAnchorFixed2>()},
+        // 64-sample blocks as two chains in z^2: closer to the Horner form's accuracy
+        {4, 128, false, 8, fwd_ptr<4, 128, kFormMixedClenEO, kAnchorFixed2>(), "mixed_clen64eo_fx2_t4_n128_s24", 0, pers_ptr<4, 128, kFormMixedClenEO, kAnchorFixed2>(), 24 * 1024},
         {2, 256, true, 8, fwd_ptr<2, 256, kFormPlain>(), "plain_t2_n256", 0, nullptr},
         {2, 128, true, 8, fwd_ptr<2, 128, kFormPlain>(), "plain_t2_n128", 0, nullptr},
         {1, 128, true, 8, fwd_ptr<1, 128, kFormPlain>(), "plain_t1_n128", 0, nullptr},

@@ -147,7 +147,7 @@ def test_deterministic_and_status_clean(cuda_dev):
     assert ops.read_status(ws) == 0
 
 
-@pytest.mark.parametrize("idx", list(range(36)))
+@pytest.mark.parametrize("idx", list(range(40)))
 def test_every_mixed_variant(cuda_dev, oracle, idx):
     from mmnorm_b200 import ops
     n = len(ops.variants("mixed"))
@@ -259,7 +259,7 @@ def test_autotuner_selects_a_variant(cuda_dev):
         ops.set_variant("mixed", 0)
 
 
-@pytest.mark.parametrize("idx", list(range(36)))
+@pytest.mark.parametrize("idx", list(range(40)))
 def test_every_mixed_variant_edge_cases(cuda_dev, oracle, idx):
     """Each mixed variant on F = 1, 33 and 100 (not multiples of the 32-sample block), on
     several RX offsets with the TI offset and a ragged antenna count, and with per-antenna
