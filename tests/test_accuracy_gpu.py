@@ -65,7 +65,7 @@ def test_accuracy_workload_subset(cuda_dev, oracle, sign):
     for mode in ("mixed", "plain"):
         I, W = _run(cuda_dev, sc, mode)
         out[mode] = _stats(oracle, I, W, idx, Io, Wo)
-    # "mixed" runs the default variant (second order, 32-sample blocks); also the variant
+    # "mixed" runs the default variant (the split second-order form); also the variant
     # the autotuner picks on this workload and the first-order Horner form
     from mmnorm_b200 import ops
     names = [v["name"] for v in ops.variants("mixed")]
