@@ -259,6 +259,23 @@ def test_autotuner_selects_a_variant(cuda_dev):
         ops.set_variant("mixed", 0)
 
 
+def test_autotuner_restricted_to_accurate_forms(cuda_dev):
+    from mmnorm_b200 import autotune, ops
+    sc = scenes.sphere_scene(seed=18, n_ap=16, nf=64, n_vox=16, n_pts=20)
+    args = [_t(v, cuda_dev) for v in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs,
+                                      np.zeros((1, 3), np.float32), sc.meas)]
+    names = [v["name"] for v in ops.variants("mixed")]
+    res = autotune.tune(*args, sc.wavelength, sc.slope, mode="mixed", max_antennas=64,
+                        candidates=autotune.ACCURATE_FORMS)
+    try:
+        timed = {names[int(i)] for i in res["times_ms"]}
+        assert timed and all(n.startswith(autotune.ACCURATE_FORMS) for n in timed)
+        assert names[res["best"]].startswith(autotune.ACCURATE_FORMS)
+        assert ops.current_variant("mixed") == res["best"]
+    finally:
+        ops.set_variant("mixed", 0)
+
+
 @pytest.mark.parametrize("idx", list(range(40)))
 def test_every_mixed_variant_edge_cases(cuda_dev, oracle, idx):
     """Each mixed variant on F = 1, 33 and 100 (not multiples of the 32-sample block), on
