@@ -135,3 +135,51 @@ def test_noalloc_just_under_its_scratch_limit(cuda_dev):
         torch.cuda.synchronize()
         assert _rel(img, ref_img) < TOL
         assert _rel(vote, ref_vote) < TOL
+
+
+def test_noalloc_records_into_a_cuda_graph(cuda_dev):
+    """The advertised real-time use: one warm call, then the call recorded into a CUDA graph
+    and replayed.  Each replay reads the inputs as they are at replay time and gives the
+    direct call's result bit for bit."""
+    import torch
+    from mmnorm_b200 import _lib, ops
+    sc = scenes.sphere_scene(seed=35, n_ap=16, nf=64, n_vox=12, n_pts=30)
+    args = _tensors(cuda_dev, sc)
+    lib = _lib.load()
+    p = ops.make_problem(*args, sc.wavelength, sc.slope)
+    V = p.num_x * p.num_y * p.num_z
+    image = torch.empty(V, dtype=torch.complex64, device=cuda_dev)
+    vote = torch.empty((3, V), dtype=torch.complex64, device=cuda_dev)
+
+    def call():
+        return lib.mmn_backproject_noalloc(ctypes.byref(p), _lib.MODES["mixed"], ops._vp(image),
+                                           ops._vp(vote), ops._stream(cuda_dev))
+
+    assert call() == _lib.MMN_OK  # warm: the context's scratch address is looked up here
+    torch.cuda.synchronize()
+    direct = (image.clone(), vote.clone())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        rc = call()
+    assert rc == _lib.MMN_OK
+    image.zero_()
+    vote.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(image, direct[0]) and torch.equal(vote, direct[1])
+
+    rng = np.random.default_rng(35)
+    new = (rng.standard_normal(sc.meas.shape)
+           + 1j * rng.standard_normal(sc.meas.shape)).astype(np.complex64)
+    args[5].copy_(torch.as_tensor(new, device=cuda_dev))
+    graph.replay()
+    torch.cuda.synchronize()
+    replayed = (image.clone(), vote.clone())
+    assert call() == _lib.MMN_OK
+    torch.cuda.synchronize()
+    assert torch.equal(replayed[0], image) and torch.equal(replayed[1], vote)
+    assert not torch.equal(replayed[0], direct[0])
+    status = ctypes.c_int32(-1)
+    assert lib.mmn_noalloc_read_status(ctypes.byref(status), ops._stream(cuda_dev)) == _lib.MMN_OK
+    assert status.value == _lib.MMN_OK
+    del graph
