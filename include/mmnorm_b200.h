@@ -32,7 +32,7 @@ extern "C" {
 
 /* status codes */
 #define MMN_OK 0
-#define MMN_ERR_INVALID_ARGUMENT 1 /* bad size, mode or flag                   */
+#define MMN_ERR_INVALID_ARGUMENT 1 /* bad size, mode, flag or array alignment  */
 #define MMN_ERR_NULL_POINTER 2     /* a required pointer is NULL               */
 #define MMN_ERR_UNSUPPORTED 3      /* device is not sm_100 / feature missing   */
 #define MMN_ERR_WORKSPACE 4        /* workspace NULL, misaligned or too small  */
@@ -56,7 +56,10 @@ extern "C" {
  * in scalar instructions.  Both give the reference's range bins and path lengths. */
 int mmn_set_interp_fast_form(int32_t form);
 
-/* Problem description.  All array pointers are device pointers. */
+/* Problem description.  All array pointers are device pointers, aligned to their
+ * element: float arrays to 4 bytes, complex64 arrays (samples, images, votes and their
+ * gradients) to 8 bytes; any other pointer returns MMN_ERR_INVALID_ARGUMENT before a
+ * device call. */
 typedef struct mmn_problem {
     int32_t num_x, num_y, num_z;  /* voxel grid                                   */
     const float *x_locs;          /* [num_x] voxel centres along x                */

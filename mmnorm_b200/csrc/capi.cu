@@ -43,6 +43,10 @@ struct FwdPlan {
 
 int variant_index_for(int mode) { return g_variant[mode == MMN_MODE_PLAIN ? 1 : 0].load(); }
 
+bool misaligned(const void *q, uintptr_t bytes) {
+    return (reinterpret_cast<uintptr_t>(q) & (bytes - 1)) != 0;
+}
+
 int check_problem(const mmn_problem *p, int mode) {
     if (!p) return MMN_ERR_NULL_POINTER;
     if (mode != MMN_MODE_MIXED && mode != MMN_MODE_PLAIN && mode != MMN_MODE_INTERP &&
@@ -59,6 +63,15 @@ int check_problem(const mmn_problem *p, int mode) {
     if (!p->x_locs || !p->y_locs || !p->z_locs) return MMN_ERR_NULL_POINTER;
     if (p->num_antennas > 0 && (!p->antenna_locs || !p->rx_offsets || !p->meas))
         return MMN_ERR_NULL_POINTER;
+    // element alignment: the kernels load float arrays as 4-byte words and a complex64
+    // sample as one 8-byte word, so a pointer off that grid is refused here rather than
+    // reaching a misaligned device load
+    if (misaligned(p->x_locs, 4) || misaligned(p->y_locs, 4) || misaligned(p->z_locs, 4) ||
+        misaligned(p->pos_offsets, 4))
+        return MMN_ERR_INVALID_ARGUMENT;
+    if (p->num_antennas > 0 && (misaligned(p->antenna_locs, 4) ||
+                                misaligned(p->rx_offsets, 4) || misaligned(p->meas, 8)))
+        return MMN_ERR_INVALID_ARGUMENT;
     return MMN_OK;
 }
 
@@ -345,6 +358,7 @@ int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vot
     int rc = check_problem(p, mode);
     if (rc != MMN_OK) return rc;
     if (!image) return MMN_ERR_NULL_POINTER;
+    if (misaligned(image, 8) || misaligned(vote, 8)) return MMN_ERR_INVALID_ARGUMENT;
     if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
         return MMN_ERR_WORKSPACE;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
@@ -357,7 +371,6 @@ int mmn_backproject(const mmn_problem *p, int32_t mode, float *image, float *vot
     unsigned char *ws = static_cast<unsigned char *>(workspace);
     if (is_interp(mode)) {
         if (workspace_bytes < kStatusBytes) return MMN_ERR_WORKSPACE;
-        if (reinterpret_cast<uintptr_t>(p->meas) & 7u) return MMN_ERR_INVALID_ARGUMENT;
         if (cudaMemsetAsync(ws, 0, 16, stream) != cudaSuccess) return MMN_ERR_CUDA;
         InterpParams ip;
         std::memset(&ip, 0, sizeof(ip));
@@ -408,6 +421,9 @@ int mmn_normals(int64_t num_voxels, const float *image, const float *vote, float
     if (num_voxels < 1) return MMN_ERR_INVALID_ARGUMENT;
     if (!image || !vote) return MMN_ERR_NULL_POINTER;
     if (!normals && !mask && !raw) return MMN_ERR_NULL_POINTER;
+    if (misaligned(image, 8) || misaligned(vote, 8) || misaligned(normals, 4) ||
+        misaligned(raw, 4))
+        return MMN_ERR_INVALID_ARGUMENT;
     if (!workspace || workspace_bytes < kStatusBytes ||
         (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
         return MMN_ERR_WORKSPACE;
@@ -425,7 +441,7 @@ int mmn_image_max_abs(int64_t num_voxels, const float *image, float *max_abs,
                       cudaStream_t stream) {
     if (num_voxels < 1) return MMN_ERR_INVALID_ARGUMENT;
     if (!image || !max_abs) return MMN_ERR_NULL_POINTER;
-    if (reinterpret_cast<uintptr_t>(max_abs) & 3) return MMN_ERR_INVALID_ARGUMENT;
+    if (misaligned(image, 8) || misaligned(max_abs, 4)) return MMN_ERR_INVALID_ARGUMENT;
     // |I| >= 0, so the float's bit pattern orders like the value: atomicMax on the bits
     cudaError_t e = launch_max_abs(num_voxels, reinterpret_cast<const float2 *>(image),
                                    reinterpret_cast<unsigned int *>(max_abs), stream);
@@ -438,7 +454,9 @@ int mmn_normals_from_max(int64_t num_voxels, const float *image, const float *vo
     if (num_voxels < 1) return MMN_ERR_INVALID_ARGUMENT;
     if (!image || !vote || !max_abs) return MMN_ERR_NULL_POINTER;
     if (!normals && !mask && !raw) return MMN_ERR_NULL_POINTER;
-    if (reinterpret_cast<uintptr_t>(max_abs) & 3) return MMN_ERR_INVALID_ARGUMENT;
+    if (misaligned(image, 8) || misaligned(vote, 8) || misaligned(max_abs, 4) ||
+        misaligned(normals, 4) || misaligned(raw, 4))
+        return MMN_ERR_INVALID_ARGUMENT;
     if (!(filter_percent >= 0.f) || !std::isfinite(filter_percent))
         return MMN_ERR_INVALID_ARGUMENT;
     cudaError_t e = launch_normals_from_max(
@@ -911,9 +929,9 @@ extern "C" int mmn_backproject_nufft(const mmn_problem *p, float *image, float *
     int rc = check_problem(p, MMN_MODE_MIXED);
     if (rc != MMN_OK) return rc;
     if (!image) return MMN_ERR_NULL_POINTER;
+    if (misaligned(image, 8) || misaligned(vote, 8)) return MMN_ERR_INVALID_ARGUMENT;
     if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
         return MMN_ERR_WORKSPACE;
-    if (reinterpret_cast<uintptr_t>(p->meas) & 7u) return MMN_ERR_INVALID_ARGUMENT;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     const int A = p->num_antennas, F = p->num_samples;
     if (A == 0) {
@@ -1018,6 +1036,9 @@ extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_
     if (rc != MMN_OK) return rc;
     if (!grad_meas && !grad_pos) return MMN_ERR_NULL_POINTER;
     if (!grad_image && !grad_vote) return MMN_ERR_NULL_POINTER;
+    if (misaligned(grad_image, 8) || misaligned(grad_vote, 8) || misaligned(grad_meas, 8) ||
+        misaligned(grad_pos, 4))
+        return MMN_ERR_INVALID_ARGUMENT;
     if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
         return MMN_ERR_WORKSPACE;
     const int A = p->num_antennas;
@@ -1236,6 +1257,7 @@ extern "C" int mmn_backproject_noalloc(const mmn_problem *p, int32_t mode, float
     int rc = check_problem(p, mode);
     if (rc != MMN_OK) return rc;
     if (!image) return MMN_ERR_NULL_POINTER;
+    if (misaligned(image, 8) || misaligned(vote, 8)) return MMN_ERR_INVALID_ARGUMENT;
     const int64_t nvox = (int64_t)p->num_x * p->num_y * p->num_z;
     FwdPlan pl;
     const bool full = !is_interp(mode) && p->num_antennas > 0;
@@ -1293,6 +1315,8 @@ extern "C" int mmn_batch_create(const mmn_problem *problems, int32_t num_objects
         const int rc = check_problem(&problems[o], mode);
         if (rc != MMN_OK) return rc;
         if (!images[o]) return MMN_ERR_NULL_POINTER;
+        if (misaligned(images[o], 8) || (votes && misaligned(votes[o], 8)))
+            return MMN_ERR_INVALID_ARGUMENT;
     }
     if (items_per_slot <= 0) items_per_slot = 8;
     int nvar = 0;

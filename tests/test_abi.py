@@ -62,6 +62,58 @@ def test_version_and_validation_without_device():
     assert h.mmn_num_variants(_lib.MODE_PLAIN) >= 1
 
 
+
+def test_misaligned_arrays_are_refused_without_device():
+    """A float array off a 4-byte boundary or a complex64 array off an 8-byte boundary is
+    refused with MMN_ERR_INVALID_ARGUMENT before any device call (the kernels load a sample
+    as one 8-byte word).  The addresses are never dereferenced."""
+    from mmnorm_b200 import _lib
+    h = _lib.load()
+    INV = _lib.MMN_ERR_INVALID_ARGUMENT
+
+    def problem(**off):
+        p = _lib.MmnProblem()
+        p.num_x = p.num_y = p.num_z = 4
+        p.num_antennas, p.num_rx, p.num_samples = 8, 1, 64
+        p.wavelength, p.slope, p.fft_spacing = 3.9e-3, 1.6e7, 2e-3
+        base = 1 << 20
+        for k, name in enumerate(("x_locs", "y_locs", "z_locs", "antenna_locs",
+                                  "rx_offsets", "meas")):
+            setattr(p, name, base + (k << 12) + off.get(name, 0))
+        return p
+
+    fake = lambda a: ctypes.c_void_p(a)
+    img, vote, ws = fake(1 << 24), fake(1 << 25), fake(1 << 26)
+    for bad in ({"meas": 4}, {"x_locs": 2}, {"antenna_locs": 1}, {"rx_offsets": 2}):
+        p = problem(**bad)
+        for mode in (_lib.MODE_MIXED, _lib.MODES["interp"]):
+            assert h.mmn_backproject(ctypes.byref(p), mode, img, vote, ws, 1 << 30, None) == INV
+            assert h.mmn_workspace_bytes(ctypes.byref(p), mode, 1) == 0
+        assert h.mmn_backproject_noalloc(ctypes.byref(p), _lib.MODE_MIXED, img, vote,
+                                         None) == INV
+        assert h.mmn_backproject_nufft(ctypes.byref(p), img, vote, ws, 1 << 30, None) == INV
+        n = ctypes.c_int32(-1)
+        assert h.mmn_plan_launches(ctypes.byref(p), _lib.MODE_MIXED, ctypes.byref(n)) == INV
+    p = problem()
+    p.pos_offsets = (1 << 21) + 2
+    assert h.mmn_backproject(ctypes.byref(p), _lib.MODE_MIXED, img, vote, ws, 1 << 30,
+                             None) == INV
+    p = problem()  # every input aligned: the outputs are checked next
+    assert h.mmn_backproject(ctypes.byref(p), _lib.MODE_MIXED, fake((1 << 24) + 4), vote, ws,
+                             1 << 30, None) == INV
+    assert h.mmn_backproject(ctypes.byref(p), _lib.MODE_MIXED, img, fake((1 << 25) + 4), ws,
+                             1 << 30, None) == INV
+    assert h.mmn_backproject_noalloc(ctypes.byref(p), _lib.MODE_MIXED, fake((1 << 24) + 4),
+                                     vote, None) == INV
+    assert h.mmn_backproject_backward(ctypes.byref(p), fake((1 << 24) + 4), None,
+                                      fake(1 << 27), None, ws, 1 << 30, None) == INV
+    assert h.mmn_backproject_backward(ctypes.byref(p), img, None, fake((1 << 27) + 4), None,
+                                      ws, 1 << 30, None) == INV
+    assert h.mmn_image_max_abs(64, fake((1 << 24) + 4), fake(1 << 27), None) == INV
+    assert h.mmn_normals(64, img, fake((1 << 25) + 4), 0.05, fake(1 << 27), None, None, ws,
+                         1 << 20, None) == INV
+
+
 def test_interpolation_form_and_probe_validation_without_device():
     """Argument checks of the interpolation-form entry points, the pass selectors and the
     wait probe, all answered before any device call."""

@@ -332,3 +332,34 @@ def test_plan_reports_its_launches(cuda_dev):
         p = ops.make_problem(*args, sc.wavelength, sc.slope)
         info = ops.plan_info(p, "mixed")
         assert info["launches"] == want + (1 if info["splits"] > 1 else 0), (nf, info)
+
+
+@pytest.mark.parametrize("idx", [0, 1])
+def test_rows_off_a_16_byte_boundary_are_staged(cuda_dev, idx):
+    """Sample rows that start 8 bytes past a 16-byte boundary (a view one sample into a
+    buffer) cannot be read in place by the bulk copies: the plan stages them (one more
+    launch) and the result is bit-identical to the same rows from an aligned buffer."""
+    import torch
+    from mmnorm_b200 import ops
+    ops.set_variant("mixed", idx)
+    try:
+        sc = small_scene(seed=71, nf=64, n_vox=16)
+        A, F = sc.meas.shape
+        axes = [_t(v, cuda_dev) for v in (sc.x_locs, sc.y_locs, sc.z_locs)]
+        ant, rxo = _t(sc.antenna_locs, cuda_dev), _t(np.zeros((1, 3), np.float32), cuda_dev)
+        aligned = _t(sc.meas, cuda_dev)
+        buf = torch.zeros(A * F + 1, dtype=torch.complex64, device=cuda_dev)
+        buf[1:].copy_(aligned.reshape(-1))
+        shifted = buf[1:].view(A, F)
+        assert aligned.data_ptr() % 16 == 0 and shifted.data_ptr() % 16 == 8
+        plans = [ops.plan_info(ops.make_problem(*axes, ant, rxo, m, sc.wavelength, sc.slope),
+                               "mixed") for m in (aligned, shifted)]
+        staged = [pl["launches"] - (1 if pl["splits"] > 1 else 0) for pl in plans]
+        if ops.variants("mixed")[idx]["name"].startswith("mixed_clen64eo_"):
+            assert staged == [2, 3], plans  # the default form reads aligned rows in place
+        outs = [ops.backproject(*axes, ant, rxo, m, sc.wavelength, sc.slope, mode="mixed")
+                for m in (aligned, shifted)]
+        torch.cuda.synchronize()
+        assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    finally:
+        ops.set_variant("mixed", 0)
