@@ -12,6 +12,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <vector>
 
@@ -45,6 +46,14 @@ int variant_index_for(int mode) { return g_variant[mode == MMN_MODE_PLAIN ? 1 : 
 
 bool misaligned(const void *q, uintptr_t bytes) {
     return (reinterpret_cast<uintptr_t>(q) & (bytes - 1)) != 0;
+}
+
+// Any of the 4-byte (float, int) arrays of the reference-signature entry points off a
+// 4-byte boundary.
+bool any_misaligned4(std::initializer_list<const void *> ptrs) {
+    for (const void *q : ptrs)
+        if (misaligned(q, 4)) return true;
+    return false;
 }
 
 int check_problem(const mmn_problem *p, int mode) {
@@ -508,6 +517,9 @@ int mmn_cuda_image(float *p_xyz_r, float *p_xyz_i, const float *x_locs, const fl
         return MMN_ERR_INVALID_ARGUMENT;
     if (num_antennas > 0 && (!antenna_locs || !meas_r || !meas_i || !rx_offsets))
         return MMN_ERR_NULL_POINTER;
+    if (any_misaligned4({p_xyz_r, p_xyz_i, x_locs, y_locs, z_locs, antenna_locs, meas_r,
+                         meas_i, rx_offsets}))
+        return MMN_ERR_INVALID_ARGUMENT;
     if (!(wavelength > 0.f)) return MMN_ERR_INVALID_ARGUMENT;
     if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)))
         return MMN_ERR_WORKSPACE;
@@ -610,6 +622,10 @@ int cuda_sn_est_impl(bool fast, float *normals_x, float *normals_y, float *norma
         return MMN_ERR_NULL_POINTER;
     if (num_antennas > 0 && (!antenna_locs || !meas_r || !meas_i || !rx_offsets))
         return MMN_ERR_NULL_POINTER;
+    if (any_misaligned4({normals_x, normals_y, normals_z, valid_idx_x, valid_idx_y,
+                         valid_idx_z, p_xyz_r, p_xyz_i, x_locs, y_locs, z_locs, antenna_locs,
+                         meas_r, meas_i, rx_offsets}))
+        return MMN_ERR_INVALID_ARGUMENT;
     if (!(wavelength > 0.f) || !(fft_spacing > 0.f)) return MMN_ERR_INVALID_ARGUMENT;
     int64_t n = count < 0 ? (int64_t)num_valid_idx - start_ind : count;
     n = std::min<int64_t>(n, (int64_t)num_valid_idx - start_ind);

@@ -112,6 +112,19 @@ def test_misaligned_arrays_are_refused_without_device():
     assert h.mmn_image_max_abs(64, fake((1 << 24) + 4), fake(1 << 27), None) == INV
     assert h.mmn_normals(64, img, fake((1 << 25) + 4), 0.05, fake(1 << 27), None, None, ws,
                          1 << 20, None) == INV
+    # the reference-signature kernels' float and int arrays: 4-byte words
+    arr = [fake((1 << 20) + (k << 12)) for k in range(16)]
+    odd = fake((1 << 28) + 2)
+    for slot in (0, 6, 8):  # p_xyz_r, meas_r, rx_offsets
+        a = list(arr[:9])
+        a[slot] = odd
+        assert h.mmn_cuda_image(*a, 1.6e7, 3.9e-3, 2e-3, 4, 4, 4, 8, 1, 64, 0, 0, 1, -1, ws,
+                                1 << 20, None) == INV
+    for slot in (0, 3, 11):  # normals_x, valid_idx_x, antenna_locs
+        a = list(arr[:15])
+        a[slot] = odd
+        assert h.mmn_cuda_sn_est(*a, 1.6e7, 3.9e-3, 2e-3, 4, 4, 4, 8, 1, 10, 64, 0, 0, -1,
+                                 ws, 1 << 20, None) == INV
 
 
 def test_interpolation_form_and_probe_validation_without_device():
