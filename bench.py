@@ -1232,7 +1232,10 @@ def accuracy_report(dev, sc, idx, sub_mixed, sub_plain, max_mixed, max_plain):
 # (a one-pass metric set, checked on the small case first), summarised in
 # profiles/bp_fwd_kernel_dram_boxcyl128.md.  Variants without a capture report null.
 FWD_DRAM_BYTES_PER_LAUNCH = {"mixed_antpair_fx2_t1_n256": 38597632 + 37433856,
-                             "mixed_clen64_fx2_t4_n128_s24": 40073728 + 36137728}
+                             "mixed_clen64_fx2_t4_n128_s24": 40073728 + 36137728,
+                             "mixed_clen64_fx2_t4_n128": 40509696 + 36157440,
+                             "mixed_clen64eo_fx2_t2_n256": 39280640 + 35329024,
+                             "mixed_clen_fx2_t4_n128_s24": 40404992 + 36330240}
 
 
 def precision_text(variant_name):
