@@ -1240,10 +1240,20 @@ FWD_DRAM_BYTES_PER_LAUNCH = {"mixed_antpair_fx2_t1_n256": 38597632 + 37433856,
 
 def precision_text(variant_name):
     """The arithmetic of a mixed-form kernel variant, for the bench line."""
-    if "clen" in variant_name:
+    if "clen64eo" in variant_name:
+        blk = 64
+        rec = ("FP32 second-order (Clenshaw) recurrence split into even- and odd-sample "
+               "chains in z^2, b_k = m_k + 2cos(2 theta) b_{k+1} - b_{k+2}, h = E + z O; "
+               "first-order Horner where |cos 2theta| > 0.98 and on a row's last partial "
+               "block")
+    elif "clen" in variant_name:
         blk = 64 if "clen64" in variant_name else 32
         rec = ("FP32 second-order (Clenshaw) rotation recurrence b_t = m_t + 2cos(theta) "
                "b_{t+1} - b_{t+2}, first-order Horner where |cos theta| > 0.98")
+    elif "split" in variant_name:
+        blk = 32
+        rec = ("FP32 first-order Horner rotation recurrence, two 16-sample chains per block "
+               "joined by z^16")
     else:
         blk = 32
         rec = "FP32 first-order Horner rotation recurrence"
