@@ -158,6 +158,7 @@ int mmn_set_measurement_pass(int32_t form);
 int mmn_num_position_variants(void);
 const char *mmn_position_variant_name(int32_t idx); /* NULL for a bad index */
 int mmn_set_position_variant(int32_t idx);
+int mmn_get_position_variant(void); /* the selected index */
 
 /*
  * Fused backprojection + vote with the per-(voxel, antenna) sample sum evaluated by

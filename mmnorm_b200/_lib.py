@@ -106,6 +106,7 @@ SIGNATURES = [
     ("mmn_num_position_variants", _I, []),
     ("mmn_position_variant_name", ctypes.c_char_p, [_I32]),
     ("mmn_set_position_variant", _I, [_I32]),
+    ("mmn_get_position_variant", _I, []),
     ("mmn_backproject_backward", _I, [_PROB, _P, _P, _P, _P, _P, _SZ, _P]),
     ("mmn_normals_workspace_bytes", _SZ, [ctypes.c_int64]),
     ("mmn_normals", _I, [ctypes.c_int64, _P, _P, _F, _P, _P, _P, _P, _SZ, _P]),

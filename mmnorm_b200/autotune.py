@@ -54,7 +54,13 @@ def tune(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slo
     ``candidates``: variant-name prefixes to consider (default: every variant), e.g.
     ``ACCURATE_FORMS`` to keep the image error near 3e-6 instead of 9e-6.
 
+    The caller's selection is kept when ``apply`` is false, and restored if timing fails.
+
     Returns {"key", "best", "times_ms": {variant index: ms}}."""
+    pool = [v for v in ops.variants(mode)
+            if candidates is None or v["name"].startswith(tuple(candidates))]
+    if not pool:
+        raise ValueError("no %s variant matches the candidates %r" % (mode, candidates))
     dev = meas.device
     nvox = x_locs.numel() * y_locs.numel() * z_locs.numel()
     key = _key(dev, mode, nvox, meas.shape[1])
@@ -72,30 +78,34 @@ def tune(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength, slo
     m = meas[sel].contiguous() if sel is not None else meas
     times = {}
     stream = torch.cuda.current_stream(dev)
-    for v in ops.variants(mode):
-        idx = v["index"]
-        if candidates is not None and not v["name"].startswith(tuple(candidates)):
-            continue
-        ops.set_variant(mode, idx)
-        ops.backproject(x_locs, y_locs, z_locs, ant, rx_offsets, m, wavelength, slope, mode=mode)
-        best = float("inf")
-        for _ in range(repeats):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
+    prev = ops.current_variant(mode)
+    try:
+        for v in pool:
+            idx = v["index"]
+            ops.set_variant(mode, idx)
             ops.backproject(x_locs, y_locs, z_locs, ant, rx_offsets, m, wavelength, slope,
                             mode=mode)
-            e1.record(stream)
-            torch.cuda.synchronize(dev)
-            best = min(best, e0.elapsed_time(e1))
-        times[idx] = best
-        if verbose:
-            print("autotune %s variant %d (%s): %.3f ms" % (mode, idx, v, best))
+            best = float("inf")
+            for _ in range(repeats):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ops.backproject(x_locs, y_locs, z_locs, ant, rx_offsets, m, wavelength, slope,
+                                mode=mode)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                best = min(best, e0.elapsed_time(e1))
+            times[idx] = best
+            if verbose:
+                print("autotune %s variant %d (%s): %.3f ms" % (mode, idx, v, best))
+    finally:
+        ops.set_variant(mode, prev)
     best_idx = min(times, key=times.get)
     res = {"key": key, "best": best_idx, "times_ms": {str(k): t for k, t in times.items()},
            "variants": ops.variants(mode), "antennas_timed": n}
     _cache[key] = res
-    ops.set_variant(mode, best_idx if apply else 0)
+    if apply:
+        ops.set_variant(mode, best_idx)
     return res
 
 
@@ -169,22 +179,27 @@ def tune_position(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavele
         ops.backproject_backward(x_locs, y_locs, z_locs, ant, rx_offsets, m, wavelength,
                                  slope, grad_image, grad_vote, want_meas=False)
 
-    for idx in range(len(names)):
-        ops.set_position_variant(idx)
-        run()
-        best = float("inf")
-        for _ in range(repeats):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
+    prev = ops.current_position_variant()
+    try:
+        for idx in range(len(names)):
+            ops.set_position_variant(idx)
             run()
-            e1.record(stream)
-            torch.cuda.synchronize(dev)
-            best = min(best, e0.elapsed_time(e1))
-        times[idx] = best
+            best = float("inf")
+            for _ in range(repeats):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                run()
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                best = min(best, e0.elapsed_time(e1))
+            times[idx] = best
+    finally:
+        ops.set_position_variant(prev)
     best_idx = min(times, key=times.get)
     res = {"key": key, "best": best_idx, "times_ms": {str(k): t for k, t in times.items()},
            "variants": names, "antennas_timed": n}
     _cache[key] = res
-    ops.set_position_variant(best_idx if apply else 0)
+    if apply:
+        ops.set_position_variant(best_idx)
     return res

@@ -1044,6 +1044,8 @@ extern "C" int mmn_set_position_variant(int32_t idx) {
     return MMN_OK;
 }
 
+extern "C" int mmn_get_position_variant(void) { return g_pos_variant.load(); }
+
 extern "C" int mmn_backproject_backward(const mmn_problem *p, const float *grad_image,
                                         const float *grad_vote, float *grad_meas,
                                         float *grad_pos, void *workspace,

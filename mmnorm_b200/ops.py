@@ -278,6 +278,11 @@ def set_position_variant(index):
     _lib.check(_lib.load().mmn_set_position_variant(int(index)), "mmn_set_position_variant")
 
 
+def current_position_variant():
+    """Index (into ``position_variants()``) of the process-wide position-pass launch shape."""
+    return int(_lib.load().mmn_get_position_variant())
+
+
 def backproject_backward(x_locs, y_locs, z_locs, antenna_locs, rx_offsets, meas, wavelength,
                          slope, grad_image, grad_vote, *, is_ti_radar=False, pos_offsets=None,
                          want_meas=True, want_pos=True):

@@ -138,6 +138,10 @@ def test_interpolation_form_and_probe_validation_without_device():
     assert h.mmn_set_measurement_pass(0) == _lib.MMN_OK
     n = h.mmn_num_position_variants()
     assert n >= 2
+    assert h.mmn_set_position_variant(n - 1) == _lib.MMN_OK
+    assert h.mmn_get_position_variant() == n - 1
+    assert h.mmn_set_position_variant(0) == _lib.MMN_OK
+    assert h.mmn_get_position_variant() == 0
     assert h.mmn_position_variant_name(0).startswith(b"interp_")
     assert h.mmn_position_variant_name(n) is None
     assert h.mmn_set_position_variant(n) == _lib.MMN_ERR_INVALID_ARGUMENT
@@ -190,3 +194,15 @@ def test_library_is_sm100a_only_build():
     """The build recipe targets exactly sm_100a."""
     from mmnorm_b200 import build
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_autotuner_refuses_candidates_that_match_no_variant():
+    """Checked before any device work, so CPU tensors suffice."""
+    import pytest
+    import torch
+    from mmnorm_b200 import autotune
+    z = torch.zeros(4)
+    with pytest.raises(ValueError):
+        autotune.tune(z, z, z, torch.zeros(2, 3), torch.zeros(1, 3),
+                      torch.zeros(2, 8, dtype=torch.complex64), 3.9e-3, 1.6e7,
+                      candidates=("no_such_form_",))

@@ -377,3 +377,21 @@ def test_position_autotuner(cuda_dev):
         assert torch.equal(gp, gp2)
     finally:
         ops.set_position_variant(0)
+
+
+def test_position_autotuner_keeps_the_callers_selection_without_apply(cuda_dev):
+    from mmnorm_b200 import autotune, ops
+    sc = scenes.sphere_scene(seed=49, n_ap=16, nf=96, n_vox=16, n_pts=20)
+    rng = np.random.default_rng(49)
+    V = sc.num_voxels
+    gI = _t((rng.standard_normal(V) + 1j * rng.standard_normal(V)).astype(np.complex64),
+            cuda_dev)
+    args = [_t(a, cuda_dev) for a in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs,
+                                      np.zeros((1, 3), np.float32), sc.meas)]
+    mine = len(ops.position_variants()) - 1
+    ops.set_position_variant(mine)
+    try:
+        autotune.tune_position(*args, sc.wavelength, sc.slope, gI, apply=False)
+        assert ops.current_position_variant() == mine
+    finally:
+        ops.set_position_variant(0)

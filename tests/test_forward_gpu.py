@@ -276,6 +276,24 @@ def test_autotuner_restricted_to_accurate_forms(cuda_dev):
         ops.set_variant("mixed", 0)
 
 
+def test_autotuner_keeps_the_callers_selection_without_apply(cuda_dev):
+    """tune(apply=False) times the variants and leaves the caller's selection in place; the
+    same call with apply (answered from the cache) selects the winner."""
+    from mmnorm_b200 import autotune, ops
+    sc = scenes.sphere_scene(seed=19, n_ap=16, nf=96, n_vox=16, n_pts=20)
+    args = [_t(v, cuda_dev) for v in (sc.x_locs, sc.y_locs, sc.z_locs, sc.antenna_locs,
+                                      np.zeros((1, 3), np.float32), sc.meas)]
+    mine = len(ops.variants("mixed")) - 1
+    ops.set_variant("mixed", mine)
+    try:
+        res = autotune.tune(*args, sc.wavelength, sc.slope, mode="mixed", max_antennas=64,
+                            apply=False)
+        assert ops.current_variant("mixed") == mine
+        again = autotune.tune(*args, sc.wavelength, sc.slope, mode="mixed", max_antennas=64)
+        assert again["best"] == res["best"] and ops.current_variant("mixed") == res["best"]
+    finally:
+        ops.set_variant("mixed", 0)
+
 @pytest.mark.parametrize("idx", list(range(40)))
 def test_every_mixed_variant_edge_cases(cuda_dev, oracle, idx):
     """Each mixed variant on F = 1, 33 and 100 (not multiples of the 32-sample block), on
